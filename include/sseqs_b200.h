@@ -1,0 +1,162 @@
+/*
+ * sseqs_b200.h -- C ABI of libsseqs_b200.so, the B200 (sm_100a) kernels of
+ * the sseqs database-search path.
+ *
+ * Conventions for every entry point:
+ *   - all pointers are device pointers unless a comment says "host";
+ *   - all work is enqueued on `stream` (0 = legacy default stream); nothing
+ *     synchronises unless a comment says so;
+ *   - the return value is a status (SSEQS_OK == 0); argument errors are
+ *     detected on the host before anything is enqueued;
+ *   - no entry point allocates device memory: scratch space is passed in as
+ *     `workspace` (size queried with the matching *_workspace_bytes call).
+ *
+ * Each declaration cites the reference interface it replaces
+ * (AlexanderMath/sseqs 0.0.8, file:line).
+ */
+#ifndef SSEQS_B200_H
+#define SSEQS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SSEQS_OK = 0,
+  SSEQS_ERR_ARG = 1,          /* invalid argument (null pointer, bad size)   */
+  SSEQS_ERR_UNSUPPORTED = 2,  /* valid input outside the supported range     */
+  SSEQS_ERR_CUDA = 3,         /* a CUDA runtime call or launch failed        */
+  SSEQS_ERR_WORKSPACE = 4     /* workspace missing or too small              */
+};
+
+/* Human-readable text for a status code (host, static storage). */
+const char* sseqs_status_string(int status);
+/* ABI version of this library. */
+int sseqs_version(void);
+/* Longest query the score kernels accept (2048). */
+int sseqs_max_query_len(void);
+
+/* ------------------------------------------------------------------ xbit */
+/* 5-bit symbol stream: 8 symbols per 5 bytes, first symbol in the high bits
+ * of a big-endian 40-bit window, symbol s <-> byte s+64 ('@' = 0 separates
+ * sequences).  Replaces decompress_launcher (sseqs/xbit.cu:65-71, kernel
+ * :8-34; torch wrapper sseqs/xbit_bind.cpp:23-28): out[0..n_syms) decodes
+ * the stream that starts at packed[lo_bytes]. */
+int sseqs_xbit_decompress(const uint8_t* packed, uint8_t* out, int64_t n_syms,
+                          int64_t lo_bytes, cudaStream_t stream);
+/* Replaces compress_launcher (sseqs/xbit.cu:73-78, kernel :36-62; wrapper
+ * sseqs/xbit_bind.cpp:11-18): out holds (5*n_syms+7)/8 bytes; a partial last
+ * group packs missing symbols as 0. */
+int sseqs_xbit_compress(const uint8_t* in, uint8_t* out, int64_t n_syms,
+                        cudaStream_t stream);
+
+/* ------------------------------------------------------ score-only SW
+ * Local alignment score of a query (class indices 0..19 in the order
+ * ARNDCQEGHILKMFPSTWYV, 1 <= query_len <= 2048) against windows of an ASCII
+ * buffer, with BLOSUM62 (non-standard target bytes score -4) and the
+ * reference's stripe rule: the horizontal dependency is cut at every query
+ * column j with j % ceil(query_len/32) == 0.
+ * Target t uses g = good_idx[t] and the window
+ *     start = starts[g-1] + 1 (starts[-1] := -1), length = starts[g]-starts[g-1]-1
+ * with result -1 when length == 0 or length < -1, and 0 when length == -1
+ * (sseqs/sw.cu:66-77, :194-204).  `ascii` must be readable through the end
+ * of every 16-byte aligned chunk that holds a byte of some window.
+ * out[t] is int32.  query_len > 2048 -> SSEQS_ERR_UNSUPPORTED. */
+
+/* Linear gap (added per gap column; the reference's msa() passes -1).
+ * Replaces launch_sw_cuda_blosum62 (sseqs/sw.cu:336-370, kernel :55-179;
+ * wrapper sseqs/sw_bind.cpp:32-73). */
+int sseqs_sw_linear(const uint8_t* query_idx, int query_len,
+                    const int32_t* good_idx, const uint8_t* ascii,
+                    const int32_t* starts, int64_t n_targets, int32_t* out,
+                    int gap, cudaStream_t stream);
+
+/* Affine gap M/Ix/Iy, gaps open from M only and the first gap column costs
+ * gap_open.  Replaces launch_sw_cuda_affine (sseqs/sw.cu:372-425, kernel
+ * :182-325; wrapper sseqs/sw_bind.cpp:78-108). */
+int sseqs_sw_affine(const uint8_t* query_idx, int query_len,
+                    const int32_t* good_idx, const uint8_t* ascii,
+                    const int32_t* starts, int64_t n_targets, int32_t* out,
+                    int gap_open, int gap_extend, cudaStream_t stream);
+
+/* Both scores above for a database batch held in HBM, in one call shape:
+ * target t is segment g = good_idx ? good_idx[t] : g0 + t of the batch whose
+ * '@' positions are `delim` (segment g = bytes between delim[g-1] and
+ * delim[g]); the first `skip` bytes of each segment are not scored.
+ * skip = 0 with delim gives the linear call of sseqs/msa.py:313-319;
+ * skip = 1 gives the affine call of sseqs/msa.py:327-332 (which passes
+ * delim+1 and so also scores the closing '@' row -- a row that can never
+ * raise a local score, so it is not computed). */
+int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
+                  const int32_t* good_idx, int32_t g0, int64_t n_targets,
+                  const uint8_t* ascii, const int32_t* delim, int skip,
+                  int32_t* out, int gap_a, int gap_b, cudaStream_t stream);
+
+/* ------------------------------------------------------------ selection */
+/* Positions (int32, increasing) of every '@' (64) byte of a decoded batch:
+ * replaces `delim_pos = arange[ascii == 64]` (sseqs/msa.py:227).  Writes at
+ * most max_out positions and the total count to *count (device int64).
+ * n must be < 2^31 (positions are batch-local int32 as in the reference). */
+size_t sseqs_find_delims_workspace_bytes(int64_t n);
+int sseqs_find_delims(const uint8_t* ascii, int64_t n, int32_t* out_pos, int64_t max_out,
+                      int64_t* count, void* workspace, size_t ws_bytes, cudaStream_t stream);
+
+/* Segment table of one decoded batch (sseqs/msa.py:237-267): with the
+ * '@' positions `delim` (*n_delims of them, device), segment k ends at
+ * delim[k] (plus a trailing segment when the batch does not end in '@');
+ * the non-empty ones are listed in order: seg_index[f] = k, lengths[f],
+ * offsets[f] = sum over earlier non-empty segments of (length+1) -- the
+ * reference's `_offsets` -- with their count in *n_segments and the largest
+ * length in *maxlen (all device).  Every output holds max_segments slots
+ * (>= number of '@' + 1). */
+size_t sseqs_segment_table_workspace_bytes(int64_t max_segments);
+int sseqs_segment_table(const uint8_t* ascii, int64_t n, const int32_t* delim,
+                        const int64_t* n_delims, int64_t max_segments, int32_t* seg_index,
+                        int32_t* lengths, int64_t* offsets, int64_t* n_segments, int32_t* maxlen,
+                        void* workspace, size_t ws_bytes, cudaStream_t stream);
+
+/* Indices (int32, increasing) of the k largest of n keys; key_type 0 =
+ * int32, 1 = IEEE half.  Ties at the k-th value are taken lowest index
+ * first.  Replaces torch.topk + torch.sort of the candidate lists
+ * (sseqs/msa.py:297, 307, 324, 335), whose tie order is unspecified.
+ * Requires 0 <= k <= n < 2^31. */
+size_t sseqs_topk_workspace_bytes(int64_t n);
+int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, int32_t* out_idx,
+               void* workspace, size_t ws_bytes, cudaStream_t stream);
+
+/* ------------------------------------------------------------ traceback */
+/* Affine local alignment with traceback of one query (raw bytes) against B
+ * targets (bytes at tbytes + toff[b], tlen[b] <= max_target_len each):
+ * replaces the Triton kernels sseqs/sw.py:408-563 (DP) and :569-768
+ * (traceback) driven by sseqs/sw.py:27-219.  Textbook Gotoh with gaps
+ * opening from H, BLOSUM62 for upper-case standard residues else -5.
+ * Outputs: best[b]; info[b*5 + 0..4] = alignment length, query start, query
+ * end, target start, target end (0-based, -1 when no alignment); the
+ * aligned query/target bytes ('-' for gaps) in the LAST `length` bytes of
+ * row b of q_aligned/t_aligned (cap >= query_len + max_target_len bytes per
+ * row).  m_full (nullable) receives M(i,j) as int32 in a [B][query_len+1]
+ * [tcols] array the caller zero-filled.  A target longer than
+ * max_target_len gets best = -1. */
+size_t sseqs_backtrack_workspace_bytes(int query_len, int max_target_len, int B);
+int sseqs_backtrack_affine(const uint8_t* query, int query_len, const uint8_t* tbytes,
+                           const int64_t* toff, const int32_t* tlen, int max_target_len, int B,
+                           int gap_open, int gap_extend, int32_t* best, int32_t* info,
+                           uint8_t* q_aligned, uint8_t* t_aligned, int cap, int32_t* m_full,
+                           int tcols, void* workspace, size_t ws_bytes, cudaStream_t stream);
+
+/* --------------------------------------------------------- diagnostics */
+/* Measured int16x2 DPX issue rate of this GPU: runs a fixed kernel of
+ * independent __viaddmax_s16x2_relu/__vimax3_s16x2 chains and writes
+ * (host) the rate in lane-instructions per second.  `sink` is one device
+ * word the kernel may write so that its work is not optimised away.
+ * Synchronises on `stream`.  No reference counterpart (measurement aid). */
+int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SSEQS_B200_H */

@@ -1,0 +1,529 @@
+// Score-only Smith-Waterman (linear and affine gaps) for sm_100a.
+//
+// Semantics are those of the reference kernels sseqs/sw.cu:55-179 (linear)
+// and sseqs/sw.cu:182-325 (affine): the query is cut into 32 stripes of
+// TPT = ceil(Lq/32) columns; inside a row the horizontal dependency restarts
+// at the first column of every stripe (H(i, j-1) := 0 there), while the
+// diagonal dependency crosses stripes.  Because the rows of all stripes are
+// independent of each other inside one row, the stripes can be evaluated in
+// any lane mapping.
+//
+// B200 mapping.  Two stripes of the same target share one 32-bit register as
+// int16x2 (lo = stripe 2m, hi = stripe 2m+1) and advance together through
+// the DPX instructions (__viaddmax_s16x2_relu, __vimax3_s16x2, ...).  A lane
+// holds W such words per column, so a target occupies G = 32/(2W) lanes and
+// a warp scores 2W targets side by side.  The query profile (score of each
+// residue class against every column, already packed as the lane's int16x2
+// words) sits in shared memory; a lane fetches its row of it with 128-bit
+// loads.  Per word-column the recurrences cost
+//   linear: max(up, left); diag + s; max(. + gap, ., 0)       -> 3 ops
+//   affine: M = max(diag + s, 0); M - open; Ix chain; D = max3(M, Ix, Iy);
+//           next-row Iy = max(Iy - ext, M - open, 0)          -> 5 ops
+// plus half a max3 for the running best.  All cell values are >= 0 and at
+// most 11 * Lq <= 22528, so int16 lanes cannot overflow for Lq <= 2048 (no
+// int32 re-run is ever needed).
+//
+// Targets are streamed: each lane group walks a contiguous range of targets,
+// reading the target bytes through 16-byte chunk loads with one chunk of
+// look-ahead, and when a target ends the group writes its score, resets its
+// state and moves on while the other groups of the warp keep going (idle
+// groups score a padding class that never raises a score).
+#include <algorithm>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace sseqs {
+
+int device_sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n > 0 ? n : 148;
+  }
+  return cached[dev];
+}
+
+namespace {
+
+constexpr int kMaxQuery = 2048;
+constexpr int kThreads = 128;
+
+struct SwArgs {
+  const uint8_t* q;       // query residue classes
+  int Lq;
+  const int32_t* idx;     // target -> window index g (nullable: g = g0 + t)
+  int32_t g0;
+  int64_t n;              // number of targets
+  const uint8_t* ascii;   // target bytes
+  const int32_t* starts;  // window table (reference semantics)
+  int skip;               // bytes not scored at the start of every window
+  int32_t* out;
+  int p0, p1;             // linear: gap; affine: open, extend
+};
+
+// Window of one target (sseqs/sw.cu:66-77): rows [pos, end), or no rows and
+// an immediate result (-1 for an empty or inverted window, 0 otherwise).
+struct Win {
+  int64_t pos, end;
+  int32_t res;
+  bool rows;
+};
+
+__device__ __forceinline__ Win window_of(const SwArgs& a, int64_t t) {
+  const int32_t g = a.idx ? a.idx[t] : (int32_t)(a.g0 + t);
+  const int64_t base = (g == 0) ? -1 : (int64_t)a.starts[g - 1];
+  const int64_t len = (int64_t)a.starts[g] - base - 1;
+  Win w;
+  w.pos = base + 1 + a.skip;
+  w.end = base + 1 + len;
+  if (len == 0 || len < -1) {
+    w.rows = false;
+    w.res = -1;
+  } else {
+    w.rows = w.pos < w.end;
+    w.res = 0;
+  }
+  return w;
+}
+
+__device__ __forceinline__ int score_of(const uint8_t* q, int Lq, int cls, int j) {
+  if (j >= Lq || cls == kClsPad) return kNeg;
+  if (cls >= kNumAA) return -4;
+  const int qc = q[j];
+  return qc < kNumAA ? blosum62(cls, qc) : -4;
+}
+
+__device__ __forceinline__ uint32_t byte_of(const uint4& c, int i) {
+  const uint32_t w = (i & 8) ? ((i & 4) ? c.w : c.z) : ((i & 4) ? c.y : c.x);
+  return (w >> ((i & 3) << 3)) & 0xffu;
+}
+
+template <int TPT>
+constexpr int words_for() {
+  return TPT == 1 ? 16 : TPT == 2 ? 8 : TPT <= 4 ? 4 : TPT <= 8 ? 2 : 1;
+}
+
+template <int TPT, int W>
+struct Layout {
+  static constexpr int G = 32 / (2 * W);    // lanes per target
+  static constexpr int GPW = 2 * W;         // targets per warp
+  static constexpr int NWD = W * TPT;       // profile words per lane and row
+  static constexpr int NV = (NWD + 3) / 4;  // 128-bit loads per lane and row
+  static constexpr int LWP = ((NV % 2) ? NV : NV + 1) * 4;  // odd # of uint4
+  static constexpr int CLS = G * LWP;       // words per residue class
+  static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
+};
+
+template <int TPT, int W, bool AFF>
+__global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
+  using L = Layout<TPT, W>;
+  constexpr int G = L::G;
+  extern __shared__ uint4 smem4[];
+  uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);
+  uint8_t* lut = reinterpret_cast<uint8_t*>(prof + kNumCls * L::CLS);
+
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = ascii_class((uint8_t)i);
+  for (int i = threadIdx.x; i < kNumCls * L::CLS; i += blockDim.x) {
+    const int c = i / L::CLS, r = i - c * L::CLS;
+    const int gl = r / L::LWP, v = r - gl * L::LWP;
+    uint32_t word = pack2(kNeg, kNeg);
+    if (v < L::NWD) {
+      const int w = v / TPT, k = v - w * TPT;
+      const int j = (gl * 2 * W + 2 * w) * TPT + k;
+      word = pack2(score_of(a.q, a.Lq, c, j), score_of(a.q, a.Lq, c, j + TPT));
+    }
+    prof[i] = word;
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / G;
+  const int gl = lane - grp * G;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t ngroups = nwarps * L::GPW;
+  const int64_t gid = wid * L::GPW + grp;
+  int64_t t = (a.n * gid) / ngroups;
+  const int64_t t_hi = (a.n * (gid + 1)) / ngroups;
+
+  const uint32_t gap2 = pack2(a.p0, a.p0);    // linear gap (<= 0)
+  const uint32_t open2 = pack2(a.p0, a.p0);   // affine open (>= 0)
+  const uint32_t next2 = pack2(-a.p1, -a.p1); // affine -extend (<= 0)
+
+  uint32_t S[W][TPT];                 // linear: H(i-1,.)  affine: D(i-1,.)
+  uint32_t Y[AFF ? W : 1][TPT];       // affine: Iy(i,.) carried into row i
+  uint32_t best = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w)
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      S[w][k] = 0;
+      if constexpr (AFF) Y[w][k] = 0;
+    }
+
+  // ---- target bookkeeping (group-uniform) ----
+  Win cur, nxt;
+  bool active = false, nxt_ok = false;
+  while (t < t_hi) {
+    cur = window_of(a, t);
+    if (cur.rows) { active = true; break; }
+    if (gl == 0) a.out[t] = cur.res;
+    ++t;
+  }
+  if (active && t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
+
+  // ---- byte stream: 16-byte chunks relative to an aligned base ----
+  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
+  const uint4* abase = reinterpret_cast<const uint4*>(au & ~(uintptr_t)15);
+  const int64_t aoff = (int64_t)(au & 15);
+  int64_t cid = -2;
+  uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
+  bool c1ok = false;
+  // A chunk is loaded only when it holds a byte that will be scored, so no
+  // load can touch memory outside the windows' 16-byte chunks.
+  auto used = [&](int64_t c) -> bool {
+    return (c << 4) < cur.end + aoff ||
+           (nxt_ok && nxt.rows && c == ((nxt.pos + aoff) >> 4));
+  };
+  auto seek = [&]() {
+    const int64_t c = (cur.pos + aoff) >> 4;
+    if (c != cid) {
+      if (c == cid + 1 && c1ok) {
+        c0 = c1;
+      } else {
+        c0 = __ldg(abase + c);
+      }
+      cid = c;
+      c1ok = false;
+    }
+    if (!c1ok && used(cid + 1)) {
+      c1 = __ldg(abase + cid + 1);
+      c1ok = true;
+    }
+  };
+  if (active) seek();
+
+  while (__any_sync(0xffffffffu, active)) {
+    int cls = kClsPad;
+    if (active) cls = lut[byte_of(c0, (int)((cur.pos + aoff) & 15))];
+
+    // ---------------- one DP row for every group of the warp ----------------
+    {
+      const uint4* pr = reinterpret_cast<const uint4*>(prof + cls * L::CLS + gl * L::LWP);
+      uint32_t s[L::NV * 4];
+#pragma unroll
+      for (int v = 0; v < L::NV; ++v) {
+        const uint4 x = pr[v];
+        s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
+      }
+      uint32_t from_left = __shfl_up_sync(0xffffffffu, S[W - 1][TPT - 1], 1, G);
+      if (gl == 0) from_left = 0;
+      uint32_t din[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w)
+        din[w] = __byte_perm(w == 0 ? from_left : S[w - 1][TPT - 1], S[w][TPT - 1], 0x5432);
+
+      uint32_t pend = 0;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        uint32_t diag = din[w];
+        if constexpr (!AFF) {
+          uint32_t left = 0;
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const uint32_t up = S[w][k];
+            const uint32_t m = (k == 0) ? up : __vmaxs2(up, left);
+            const uint32_t u = __vadd2(diag, s[w * TPT + k]);
+            const uint32_t h = __viaddmax_s16x2_relu(m, gap2, u);
+            diag = up;
+            S[w][k] = h;
+            left = h;
+            if (((w * TPT + k) & 1) == 0) pend = h;
+            else best = __vimax3_s16x2(best, pend, h);
+          }
+        } else {
+          uint32_t X = 0, mo_left = 0;
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            const uint32_t M = __viaddmax_s16x2_relu(diag, s[w * TPT + k], 0u);
+            const uint32_t mo = __vsub2(M, open2);
+            if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
+            const uint32_t y = Y[w][k];
+            const uint32_t D = __vimax3_s16x2(M, X, y);
+            Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
+            diag = S[w][k];
+            S[w][k] = D;
+            mo_left = mo;
+            if (((w * TPT + k) & 1) == 0) pend = D;
+            else best = __vimax3_s16x2(best, pend, D);
+          }
+        }
+      }
+      if ((L::NWD & 1) != 0) best = __vmaxs2(best, pend);
+    }
+
+    if (active) {
+      ++cur.pos;
+      if (cur.pos == cur.end) {
+        // target finished: reduce the group's best, reset, move on
+        int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
+        if (gl == 0) a.out[t] = v;
+        best = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+#pragma unroll
+          for (int k = 0; k < TPT; ++k) {
+            S[w][k] = 0;
+            if constexpr (AFF) Y[w][k] = 0;
+          }
+        ++t;
+        active = false;
+        if (t < t_hi) {
+          cur = nxt_ok ? nxt : window_of(a, t);
+          nxt_ok = false;
+          while (!cur.rows) {
+            if (gl == 0) a.out[t] = cur.res;
+            if (++t >= t_hi) break;
+            cur = window_of(a, t);
+          }
+          if (t < t_hi) {
+            active = true;
+            if (t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
+            seek();
+          }
+        }
+      } else if (((cur.pos + aoff) & 15) == 0) {
+        seek();
+      }
+    }
+  }
+}
+
+// Exact restatement for gap parameters outside the fast kernel's domain
+// (linear gap > 0, affine open/extend < 0): one thread per target, cells
+// stored as uint16 (linear) / int16 (affine) exactly as sseqs/sw.cu does.
+__global__ void sw_generic_kernel(SwArgs a, int affine) {
+  uint16_t h[kMaxQuery];
+  int16_t xm[kMaxQuery], xx[kMaxQuery], xy[kMaxQuery];
+  const int TPT = (a.Lq + 31) / 32;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const Win w = window_of(a, t);
+    if (!w.rows) { a.out[t] = w.res; continue; }
+    int best = 0;
+    for (int j = 0; j < a.Lq; ++j) { h[j] = 0; xm[j] = xx[j] = xy[j] = 0; }
+    for (int64_t p = w.pos; p < w.end; ++p) {
+      const int c = ascii_class(a.ascii[p]);
+      if (!affine) {
+        int diag = 0, left = 0;
+        for (int j = 0; j < a.Lq; ++j) {
+          const int s = score_of(a.q, a.Lq, c, j);
+          const int up = h[j];
+          if (j % TPT == 0) left = 0;
+          int v = max(0, max(diag + s, max(up + a.p0, left + a.p0)));
+          const uint16_t v16 = (uint16_t)v;
+          diag = up;
+          h[j] = v16;
+          left = v16;
+          best = max(best, (int)v16);
+        }
+      } else {
+        int dm = 0, dx = 0, dy = 0, lm = 0, lx = 0;
+        for (int j = 0; j < a.Lq; ++j) {
+          const int s = score_of(a.q, a.Lq, c, j);
+          if (j % TPT == 0) { lm = 0; lx = 0; }
+          const int um = xm[j], ux = xx[j], uy = xy[j];
+          const int16_t m = (int16_t)max(0, max(dm + s, max(dx + s, dy + s)));
+          const int16_t x = (int16_t)max(0, max(lm - a.p0, lx - a.p1));
+          const int16_t y = (int16_t)max(0, max(um - a.p0, uy - a.p1));
+          dm = um; dx = ux; dy = uy;
+          xm[j] = m; xx[j] = x; xy[j] = y;
+          lm = m; lx = x;
+          best = max(best, max((int)m, max((int)x, (int)y)));
+        }
+      }
+    }
+    a.out[t] = best;
+  }
+}
+
+__global__ void fill_kernel(int32_t* out, int64_t n, int32_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = v;
+}
+
+// ---------------------------------------------------------------- dispatch
+using KernelFn = void (*)(SwArgs);
+
+struct KernelInfo {
+  KernelFn fn = nullptr;
+  size_t smem = 0;
+  int groups_per_block = 0;
+};
+
+template <int TPT, bool AFF>
+KernelInfo make_info() {
+  constexpr int W = words_for<TPT>();
+  KernelInfo k;
+  k.fn = sw_stream_kernel<TPT, W, AFF>;
+  k.smem = Layout<TPT, W>::smem;
+  k.groups_per_block = (kThreads / 32) * Layout<TPT, W>::GPW;
+  return k;
+}
+
+template <bool AFF, int... T>
+void fill_table(KernelInfo* tab, std::integer_sequence<int, T...>) {
+  ((tab[T] = make_info<T + 1, AFF>()), ...);
+}
+
+struct Cache {
+  std::mutex mu;
+  int max_blocks[2][64][64] = {};  // [affine][TPT-1][device]
+};
+Cache& cache() {
+  static Cache c;
+  return c;
+}
+
+const KernelInfo& info_for(int tpt, bool aff) {
+  static KernelInfo lin[64], afn[64];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    fill_table<false>(lin, std::make_integer_sequence<int, 64>{});
+    fill_table<true>(afn, std::make_integer_sequence<int, 64>{});
+  });
+  return aff ? afn[tpt - 1] : lin[tpt - 1];
+}
+
+int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
+  const int tpt = (a.Lq + 31) / 32;
+  const KernelInfo& k = info_for(tpt, aff);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
+  int blocks_per_sm;
+  {
+    std::lock_guard<std::mutex> lk(cache().mu);
+    int& mb = cache().max_blocks[aff][tpt - 1][dev];
+    if (mb == 0) {
+      if (cudaFuncSetAttribute((const void*)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)k.smem) != cudaSuccess)
+        return SSEQS_ERR_CUDA;
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)k.fn, kThreads,
+                                                        k.smem) != cudaSuccess || nb < 1)
+        return SSEQS_ERR_CUDA;
+      mb = nb;
+    }
+    blocks_per_sm = mb;
+  }
+  const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
+  const int64_t need = (a.n + k.groups_per_block - 1) / k.groups_per_block;
+  const int grid = (int)std::max<int64_t>(1, std::min(full, need));
+  k.fn<<<grid, kThreads, k.smem, stream>>>(a);
+  return status_of(cudaGetLastError());
+}
+
+int run(bool aff, SwArgs a, cudaStream_t stream) {
+  if (a.n < 0 || (a.n > 0 && (!a.out || !a.starts || !a.ascii))) return SSEQS_ERR_ARG;
+  if (a.n == 0) return SSEQS_OK;
+  if (a.Lq < 0) return SSEQS_ERR_ARG;
+  if (a.Lq > kMaxQuery) return SSEQS_ERR_UNSUPPORTED;
+  if (a.Lq == 0) {   // sseqs/sw.cu:73: every result is -1
+    const int grid = (int)std::min<int64_t>((a.n + 255) / 256, 4096);
+    fill_kernel<<<grid, 256, 0, stream>>>(a.out, a.n, -1);
+    return status_of(cudaGetLastError());
+  }
+  if (!a.q) return SSEQS_ERR_ARG;
+  const bool fast = aff ? (a.p0 >= 0 && a.p1 >= 0) : (a.p0 <= 0);
+  if (fast) {
+    a.p0 = aff ? std::min(a.p0, 32767) : std::max(a.p0, -32768);
+    a.p1 = std::min(a.p1, 32767);
+    return launch_stream(a, aff, stream);
+  }
+  if (a.skip != 0) return SSEQS_ERR_UNSUPPORTED;
+  const int grid = (int)std::min<int64_t>((a.n + 127) / 128, (int64_t)device_sm_count() * 4);
+  sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0);
+  return status_of(cudaGetLastError());
+}
+
+// ------------------------------------------------------- DPX peak probe
+__global__ void dpx_peak_kernel(uint32_t* sink, int iters, uint32_t seed) {
+  uint32_t x[8], y[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    x[i] = seed * (threadIdx.x + 7 * i + 1);
+    y[i] = seed ^ (blockIdx.x + 13 * i);
+  }
+  const uint32_t d = seed | 0x00010001u, e = seed >> 3;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      x[i] = __viaddmax_s16x2_relu(x[i], d, y[i]);
+      y[i] = __vimax3_s16x2(y[i], x[i], e);
+    }
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc ^= x[i] ^ y[i];
+  if (acc == 0x9e3779b9u) sink[0] = acc;   // practically never taken
+}
+
+}  // namespace
+}  // namespace sseqs
+
+using namespace sseqs;
+
+extern "C" int sseqs_max_query_len(void) { return kMaxQuery; }
+
+extern "C" int sseqs_sw_linear(const uint8_t* query_idx, int query_len, const int32_t* good_idx,
+                               const uint8_t* ascii, const int32_t* starts, int64_t n_targets,
+                               int32_t* out, int gap, cudaStream_t stream) {
+  if (!good_idx && n_targets > 0) return SSEQS_ERR_ARG;
+  SwArgs a{query_idx, query_len, good_idx, 0, n_targets, ascii, starts, 0, out, gap, 0};
+  return run(false, a, stream);
+}
+
+extern "C" int sseqs_sw_affine(const uint8_t* query_idx, int query_len, const int32_t* good_idx,
+                               const uint8_t* ascii, const int32_t* starts, int64_t n_targets,
+                               int32_t* out, int gap_open, int gap_extend, cudaStream_t stream) {
+  if (!good_idx && n_targets > 0) return SSEQS_ERR_ARG;
+  SwArgs a{query_idx, query_len, good_idx, 0, n_targets, ascii, starts, 0, out, gap_open, gap_extend};
+  return run(true, a, stream);
+}
+
+extern "C" int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
+                             const int32_t* good_idx, int32_t g0, int64_t n_targets,
+                             const uint8_t* ascii, const int32_t* delim, int skip, int32_t* out,
+                             int gap_a, int gap_b, cudaStream_t stream) {
+  if (skip < 0 || g0 < 0) return SSEQS_ERR_ARG;
+  SwArgs a{query_idx, query_len, good_idx, g0, n_targets, ascii, delim, skip, out, gap_a, gap_b};
+  return run(affine != 0, a, stream);
+}
+
+extern "C" int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream) {
+  if (!lane_ops_per_s || !sink) return SSEQS_ERR_ARG;
+  const int blocks = device_sm_count() * 8, threads = 256, iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return SSEQS_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return SSEQS_ERR_CUDA; }
+  dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters / 8, 0x12345u);   // warm-up
+  cudaEventRecord(e0, stream);
+  dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters, 0x12345u);
+  cudaEventRecord(e1, stream);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess || ms <= 0.f) return SSEQS_ERR_CUDA;
+  *lane_ops_per_s = (double)blocks * threads * iters * 16.0 / (ms * 1e-3);
+  return SSEQS_OK;
+}

@@ -1,0 +1,138 @@
+"""GPU parity of the score kernels: CUDA vs the CPU oracle vs the reference's
+own CUDA kernels, bit-exact (int32 scores)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests import refkernels
+from tests.helpers import homolog_targets, rand_seq
+
+pytestmark = pytest.mark.gpu
+NT = os.cpu_count() or 4
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _case(seed, Lq, n_targets, extra=""):
+    rng = np.random.default_rng(seed)
+    query = rand_seq(rng, Lq)
+    targets = homolog_targets(rng, query, n_targets, lo=1, hi=400)
+    if extra:
+        targets += [rand_seq(rng, int(rng.integers(1, 80)), extra=extra) for _ in range(8)]
+    ascii, starts = O.pack_targets(targets)
+    return query, O.encode_query(query), ascii, starts
+
+
+QUERY_LENGTHS = [1, 2, 17, 32, 33, 64, 65, 100, 128, 129, 200, 256, 257, 300, 500, 511, 640,
+                 777, 1000, 1024, 1025, 1500, 2048]
+
+
+@pytest.mark.parametrize("Lq", QUERY_LENGTHS)
+def test_sw_ops_match_oracle(Lq):
+    from sseqs_b200 import sw as S
+    n = 600 if Lq <= 300 else (250 if Lq <= 1024 else 120)
+    query, q, ascii, starts = _case(Lq, Lq, n, extra="XBZU*@")
+    good = np.arange(len(starts), dtype=np.int32)
+    rng = np.random.default_rng(Lq + 7)
+    good = rng.permutation(good)            # arbitrary order, includes g = 0
+    qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
+    lin = S.sw_cuda_blosum62(qd, gd, ad, sd, gap_penalty_param=-1).cpu().numpy()
+    np.testing.assert_array_equal(lin, O.sw_linear(q, good, ascii, starts, -1, NT))
+    aff = S.sw_cuda_affine(qd, gd, ad, sd, 11, 1).cpu().numpy()
+    np.testing.assert_array_equal(aff, O.sw_affine(q, good, ascii, starts, 11, 1, NT))
+    # the msa() affine call passes delimiter+1 so windows skip one residue and
+    # end on the '@'
+    sp = (starts + 1).astype(np.int32)
+    aff2 = S.sw_cuda_affine(qd, gd, ad, _dev(sp), 11, 1).cpu().numpy()
+    np.testing.assert_array_equal(aff2, O.sw_affine(q, good, ascii, sp, 11, 1, NT))
+
+
+@pytest.mark.parametrize("Lq", [40, 200, 513, 1024])
+def test_sw_ops_match_reference_cuda_kernels(Lq):
+    if not refkernels.available():
+        pytest.skip("oracle/_ref/libsseqs_ref.so not built")
+    from sseqs_b200 import sw as S
+    query, q, ascii, starts = _case(1000 + Lq, Lq, 700, extra="XB")
+    good = np.arange(1, len(starts), dtype=np.int32)     # g >= 1: defined windows
+    qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
+    for gap in (-1, -4, -11):
+        mine = S.sw_cuda_blosum62(qd, gd, ad, sd, gap_penalty_param=gap)
+        ref = refkernels.sw_linear(qd, gd, ad, sd, gap)
+        torch.testing.assert_close(mine, ref, rtol=0, atol=0)
+    for go, ge in ((11, 1), (5, 2), (0, 0)):
+        mine = S.sw_cuda_affine(qd, gd, ad, sd, go, ge)
+        ref = refkernels.sw_affine(qd, gd, ad, sd, go, ge)
+        torch.testing.assert_close(mine, ref, rtol=0, atol=0)
+    sp = _dev((starts + 1).astype(np.int32))
+    torch.testing.assert_close(S.sw_cuda_affine(qd, gd, ad, sp, 11, 1),
+                               refkernels.sw_affine(qd, gd, ad, sp, 11, 1), rtol=0, atol=0)
+
+
+def test_scan_matches_reference_windows():
+    """sw_scan over a decoded batch == the two window forms msa() uses."""
+    from sseqs_b200 import sw as S
+    query, q, ascii, starts = _case(77, 333, 3000)
+    pad = np.full(100, 64, np.uint8)             # '@' padding as in a packed chunk
+    ascii = np.concatenate([ascii, pad])
+    delim = np.flatnonzero(ascii == 64).astype(np.int32)
+    nseg = len(starts)
+    qd, ad, dd = _dev(q), _dev(ascii), _dev(delim)
+    good = np.arange(1, nseg - 1, dtype=np.int32)
+    gd = _dev(good)
+    lin = S.sw_scan(qd, ad, dd, affine=False, good_idx=gd, skip=0, gap_a=-1)
+    lin_ref = S.sw_cuda_blosum62(qd, gd, ad, dd, gap_penalty_param=-1)
+    torch.testing.assert_close(lin, lin_ref, rtol=0, atol=0)
+    sp = _dev((delim + 1).astype(np.int32))
+    aff = S.sw_scan(qd, ad, dd, affine=True, good_idx=gd, skip=1, gap_a=11, gap_b=1)
+    aff_ref = S.sw_cuda_affine(qd, gd, ad, sp, 11, 1)
+    torch.testing.assert_close(aff, aff_ref, rtol=0, atol=0)
+    # implicit target range (whole batch), g0 offset
+    full = S.sw_scan(qd, ad, dd, affine=True, g0=1, n_targets=nseg - 2, skip=1, gap_a=11, gap_b=1)
+    torch.testing.assert_close(full, aff_ref, rtol=0, atol=0)
+    np.testing.assert_array_equal(
+        full.cpu().numpy(), O.sw_affine(q, good, ascii, delim + 1, 11, 1, NT))
+
+
+def test_nonstandard_gap_parameters_use_exact_generic_path():
+    from sseqs_b200 import sw as S
+    query, q, ascii, starts = _case(5, 90, 200)
+    good = np.arange(len(starts), dtype=np.int32)
+    qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
+    np.testing.assert_array_equal(S.sw_cuda_blosum62(qd, gd, ad, sd, 2).cpu().numpy(),
+                                  O.sw_linear(q, good, ascii, starts, 2, NT))
+    np.testing.assert_array_equal(S.sw_cuda_affine(qd, gd, ad, sd, -3, 1).cpu().numpy(),
+                                  O.sw_affine(q, good, ascii, starts, -3, 1, NT))
+
+
+def test_degenerate_inputs():
+    from sseqs_b200 import sw as S
+    q = _dev(O.encode_query("MKTAYIAKQRQ"))
+    ascii = _dev(np.frombuffer(b"MKTAYIAK@@QRQ@W@", np.uint8).copy())
+    starts = np.array([8, 9, 13, 15, 15, 3], np.int32)
+    good = np.arange(6, dtype=np.int32)
+    out = S.sw_cuda_affine(q, _dev(good), ascii, _dev(starts)).cpu().numpy()
+    np.testing.assert_array_equal(out, O.sw_affine(O.encode_query("MKTAYIAKQRQ"), good,
+                                                   ascii.cpu().numpy(), starts))
+    empty = torch.zeros(0, dtype=torch.uint8, device="cuda")
+    assert (S.sw_cuda_blosum62(empty, _dev(good), ascii, _dev(starts)) == -1).all()
+    none = S.sw_cuda_affine(q, _dev(np.zeros(0, np.int32)), ascii, _dev(starts))
+    assert none.numel() == 0
+    with pytest.raises(RuntimeError):
+        S.sw_cuda_affine(_dev(np.zeros(2049, np.uint8)), _dev(good), ascii, _dev(starts))
+
+
+def test_sw_api_matches_oracle():
+    import sseqs_b200
+    rng = np.random.default_rng(3)
+    query = rand_seq(rng, 150)
+    targets = homolog_targets(rng, query, 50, lo=3, hi=200)
+    got = sseqs_b200.sw(query, targets).cpu().numpy()
+    ascii, starts = O.pack_targets(targets)
+    exp = O.sw_affine(O.encode_query(query), np.arange(len(targets), dtype=np.int32),
+                      ascii, starts, 11, 1)
+    np.testing.assert_array_equal(got, exp)

@@ -1,0 +1,62 @@
+"""CPU checks of the C ABI library: it loads and exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "sseqs_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sseqs_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from sseqs_b200 import build
+    path = build.build()
+    return ctypes.CDLL(path)
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    names = _declared()
+    assert len(names) >= 10
+    for name in names:
+        assert hasattr(built_lib, name), name
+
+
+def test_python_binding_covers_declared_symbols():
+    from sseqs_b200 import _lib
+    assert set(_declared()) <= set(_lib.exported_symbols())
+
+
+def test_status_strings_and_limits(built_lib):
+    from sseqs_b200 import _lib
+    L = _lib.lib()
+    assert L.sseqs_status_string(0) == b"ok"
+    assert b"workspace" in L.sseqs_status_string(4)
+    assert L.sseqs_max_query_len() == 2048
+    assert L.sseqs_version() >= 1
+
+
+def test_argument_errors_are_reported_without_a_gpu(built_lib):
+    """Host-side argument checks run before any CUDA call."""
+    from sseqs_b200 import _lib
+    L = _lib.lib()
+    assert L.sseqs_topk(None, 0, 10, 11, None, None, 0, None) == 1        # k > n
+    assert L.sseqs_topk(None, 5, 10, 1, None, None, 0, None) == 1         # bad key type
+    assert L.sseqs_xbit_decompress(None, None, -1, 0, None) == 1
+    assert L.sseqs_sw_scan(1, None, 10, None, -1, 5, None, None, 0, None, 11, 1, None) == 1
+    assert L.sseqs_find_delims(None, 10, None, 0, None, None, 0, None) == 1
+    assert L.sseqs_backtrack_workspace_bytes(10, 20, 2) > 0
+
+
+def test_fails_loudly_without_library(monkeypatch, tmp_path):
+    from sseqs_b200 import _lib
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(ImportError):
+        _lib.lib()
