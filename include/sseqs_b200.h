@@ -128,6 +128,14 @@ size_t sseqs_topk_workspace_bytes(int64_t n);
 int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, int32_t* out_idx,
                void* workspace, size_t ws_bytes, cudaStream_t stream);
 
+/* Hit strings of selected segments: row r of out (width bytes) receives
+ * ascii[offsets[g] .. offsets[g] + min(width, lengths[g])), g = idx[r], the
+ * rest of the row zero, and out_len[r] the copied length.  Replaces the
+ * gather of sseqs/msa.py:349-370 (width 500 there, sseqs/msa.py:183). */
+int sseqs_gather_windows(const uint8_t* ascii, const int64_t* offsets, const int32_t* lengths,
+                         const int32_t* idx, int64_t n, int width, uint8_t* out,
+                         int32_t* out_len, cudaStream_t stream);
+
 /* ------------------------------------------------------------ traceback */
 /* Affine local alignment with traceback of one query (raw bytes) against B
  * targets (bytes at tbytes + toff[b], tlen[b] <= max_target_len each):
@@ -148,6 +156,21 @@ int sseqs_backtrack_affine(const uint8_t* query, int query_len, const uint8_t* t
                            uint8_t* q_aligned, uint8_t* t_aligned, int cap, int32_t* m_full,
                            int tcols, void* workspace, size_t ws_bytes, cudaStream_t stream);
 
+/* ------------------------------------------------------------ prefilter */
+/* Gapless rank-k correlation score of every segment (fp16 out[s]):
+ * 0.5 * max over even lags of sum_r (a_r (*) b_r), a cyclic convolution of
+ * length n (power of two, 64..2048), a_r[i] = lut_a[r][query_pos_reversed[i]],
+ * b_r[i] = lut_b[r][pos(t[i])] over the segment's bytes ascii[offsets[s] ..
+ * + lengths[s]); lut_a / lut_b are float [k][21] (k <= 20).  Replaces
+ * launch_warp_corr (sseqs/filter.cu:161-395 with kernels
+ * sseqs/filter.cu:92-159 and sseqs/fft.cu:17-415, wrapper
+ * sseqs/filter_bind.cpp:20-64); computed in fp32. */
+size_t sseqs_prefilter_workspace_bytes(int n, int k);
+int sseqs_prefilter(const uint8_t* ascii, const int64_t* offsets, const int32_t* lengths,
+                    int64_t n_segments, const uint8_t* query_pos_reversed, int query_len,
+                    const float* lut_a, const float* lut_b, int k, int n, void* out,
+                    void* workspace, size_t ws_bytes, cudaStream_t stream);
+
 /* --------------------------------------------------------- diagnostics */
 /* Measured int16x2 DPX issue rate of this GPU: runs a fixed kernel of
  * independent __viaddmax_s16x2_relu/__vimax3_s16x2 chains and writes
@@ -155,6 +178,9 @@ int sseqs_backtrack_affine(const uint8_t* query, int query_len, const uint8_t* t
  * word the kernel may write so that its work is not optimised away.
  * Synchronises on `stream`.  No reference counterpart (measurement aid). */
 int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream);
+/* Number of kernels this library has enqueued since it was loaded (every
+ * launch site counts itself).  No reference counterpart. */
+int64_t sseqs_launch_count(void);
 
 #ifdef __cplusplus
 }

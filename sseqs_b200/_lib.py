@@ -37,10 +37,14 @@ _SIGNATURES = {
     "sseqs_segment_table": (_I, [_P, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "sseqs_topk_workspace_bytes": (_SZ, [_I64]),
     "sseqs_topk": (_I, [_P, _I, _I64, _I64, _P, _P, _SZ, _P]),
+    "sseqs_gather_windows": (_I, [_P, _P, _P, _P, _I64, _I, _P, _P, _P]),
     "sseqs_backtrack_workspace_bytes": (_SZ, [_I, _I, _I]),
     "sseqs_backtrack_affine": (_I, [_P, _I, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I,
                                     _P, _I, _P, _SZ, _P]),
+    "sseqs_prefilter_workspace_bytes": (_SZ, [_I, _I]),
+    "sseqs_prefilter": (_I, [_P, _P, _P, _I64, _P, _I, _P, _P, _I, _I, _P, _P, _SZ, _P]),
     "sseqs_dpx_peak": (_I, [_P, ctypes.POINTER(_D), _P]),
+    "sseqs_launch_count": (_I64, []),
 }
 
 _lock = threading.Lock()
@@ -94,6 +98,21 @@ def require_cuda(*tensors) -> None:
     for t in tensors:
         if t is not None and not t.is_cuda:
             raise ValueError("sseqs_b200 operations take CUDA tensors")
+
+
+# Bytes moved between host and device by the package's own transfer points
+# (queries and traceback inputs in, hits and alignments out).
+transfer_bytes = {"h2d": 0, "d2h": 0}
+
+
+def to_device(t: torch.Tensor, device="cuda") -> torch.Tensor:
+    transfer_bytes["h2d"] += t.numel() * t.element_size()
+    return t.to(device)
+
+
+def to_host(t: torch.Tensor):
+    transfer_bytes["d2h"] += t.numel() * t.element_size()
+    return t.cpu().numpy()
 
 
 def workspace(nbytes: int, device) -> torch.Tensor:

@@ -1,5 +1,14 @@
-// Library-wide entry points: status text and ABI version.
+// Library-wide entry points: status text, ABI version, launch counter.
+#include <atomic>
+
 #include "common.cuh"
+
+namespace sseqs {
+namespace {
+std::atomic<long long> g_launches{0};
+}
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace sseqs
 
 extern "C" const char* sseqs_status_string(int status) {
   switch (status) {
@@ -13,3 +22,5 @@ extern "C" const char* sseqs_status_string(int status) {
 }
 
 extern "C" int sseqs_version(void) { return 1; }
+
+extern "C" int64_t sseqs_launch_count(void) { return sseqs::g_launches.load(); }

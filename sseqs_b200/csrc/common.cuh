@@ -71,4 +71,7 @@ inline int status_of(cudaError_t e) { return e == cudaSuccess ? SSEQS_OK : SSEQS
 // Number of SMs of the current device (cached per device ordinal).
 int device_sm_count();
 
+// Adds n to the library-wide count of kernel launches (sseqs_launch_count).
+void count_launches(int n);
+
 }  // namespace sseqs

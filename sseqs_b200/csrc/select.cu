@@ -334,6 +334,21 @@ __global__ void exclusive_apply_kernel(int64_t* data, int64_t n, const int64_t* 
   }
 }
 
+// out[r][0..width) = ascii[offsets[g] + c] for c < min(width, lengths[g]),
+// g = idx[r]; out_len[r] = min(width, lengths[g]).
+__global__ void gather_windows_kernel(const uint8_t* ascii, const int64_t* offsets,
+                                      const int32_t* lengths, const int32_t* idx, int64_t n,
+                                      int width, uint8_t* out, int32_t* out_len) {
+  for (int64_t r = blockIdx.x; r < n; r += gridDim.x) {
+    const int32_t g = idx[r];
+    const int64_t off = offsets[g];
+    const int len = min(width, (int)lengths[g]);
+    for (int c = threadIdx.x; c < width; c += blockDim.x)
+      out[r * width + c] = c < len ? ascii[off + c] : (uint8_t)0;
+    if (threadIdx.x == 0) out_len[r] = len;
+  }
+}
+
 inline int grid_for(int64_t n) {
   const int64_t tiles = (n + kTile - 1) / kTile;
   return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)device_sm_count() * 8));
@@ -363,9 +378,9 @@ extern "C" int sseqs_find_delims(const uint8_t* ascii, int64_t n, int32_t* out_p
   const int64_t tiles = (n + kTile - 1) / kTile;
   const int grid = grid_for(n);
   IsByte pred{ascii, 64};
-  count_kernel<<<grid, kSelThreads, 0, stream>>>(pred, n, cnt);
-  scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cnt, tiles, count);
-  scatter_kernel<<<grid, kSelThreads, 0, stream>>>(pred, n, cnt, out_pos, max_out, nullptr, nullptr);
+  { count_kernel<<<grid, kSelThreads, 0, stream>>>(pred, n, cnt); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cnt, tiles, count); count_launches(1); }
+  { scatter_kernel<<<grid, kSelThreads, 0, stream>>>(pred, n, cnt, out_pos, max_out, nullptr, nullptr); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -402,17 +417,17 @@ extern "C" int sseqs_segment_table(const uint8_t* ascii, int64_t n, const int32_
   cudaMemsetAsync(all_len, 0, sizeof(int32_t) * (size_t)max_segments, stream);
   cudaMemsetAsync(maxlen, 0, sizeof(int32_t), stream);
   // all segments (the reference's `lengths` before filtering)
-  seg_lengths_kernel<<<grid, kSelThreads, 0, stream>>>(delim, n_delims, n, ascii, all_len, nall);
+  { seg_lengths_kernel<<<grid, kSelThreads, 0, stream>>>(delim, n_delims, n, ascii, all_len, nall); count_launches(1); }
   NonZero nz{all_len};
-  count_kernel<<<grid, kSelThreads, 0, stream>>>(nz, max_segments, cnt);
-  scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cnt, tiles, n_segments);
-  scatter_kernel<<<grid, kSelThreads, 0, stream>>>(nz, max_segments, cnt, seg_index, max_segments,
-                                                  nullptr, nullptr);
-  gather_lengths_kernel<<<grid, kSelThreads, 0, stream>>>(all_len, seg_index, n_segments, lengths,
-                                                         offsets, maxlen);
-  exclusive_tiles_kernel<<<grid, kSelThreads, 0, stream>>>(offsets, max_segments, tsum);
-  scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(tsum, tiles, nullptr);
-  exclusive_apply_kernel<<<grid, kSelThreads, 0, stream>>>(offsets, max_segments, tsum);
+  { count_kernel<<<grid, kSelThreads, 0, stream>>>(nz, max_segments, cnt); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cnt, tiles, n_segments); count_launches(1); }
+  { scatter_kernel<<<grid, kSelThreads, 0, stream>>>(nz, max_segments, cnt, seg_index, max_segments,
+                                                  nullptr, nullptr); count_launches(1); }
+  { gather_lengths_kernel<<<grid, kSelThreads, 0, stream>>>(all_len, seg_index, n_segments, lengths,
+                                                         offsets, maxlen); count_launches(1); }
+  { exclusive_tiles_kernel<<<grid, kSelThreads, 0, stream>>>(offsets, max_segments, tsum); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(tsum, tiles, nullptr); count_launches(1); }
+  { exclusive_apply_kernel<<<grid, kSelThreads, 0, stream>>>(offsets, max_segments, tsum); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -429,7 +444,7 @@ extern "C" int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, 
   if (!keys || !out_idx) return SSEQS_ERR_ARG;
   if (n > INT32_MAX) return SSEQS_ERR_UNSUPPORTED;
   if (k == n) {
-    iota_kernel<<<grid_for(n), kSelThreads, 0, stream>>>(out_idx, n);
+    { iota_kernel<<<grid_for(n), kSelThreads, 0, stream>>>(out_idx, n); count_launches(1); }
     return status_of(cudaGetLastError());
   }
   if (!workspace || ws_bytes < sseqs_topk_workspace_bytes(n)) return SSEQS_ERR_WORKSPACE;
@@ -443,20 +458,34 @@ extern "C" int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, 
   const int grid = grid_for(n);
   const int hgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + kSelThreads - 1) / kSelThreads,
                                                                 (int64_t)device_sm_count() * 4));
-  topk_init_kernel<<<1, 256, 0, stream>>>(ctl, k);
+  { topk_init_kernel<<<1, 256, 0, stream>>>(ctl, k); count_launches(1); }
   const int first_shift = key_type == 0 ? 24 : 8;
   for (int shift = first_shift; shift >= 0; shift -= 8) {
     if (key_type == 0)
-      topk_hist_kernel<0><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift);
+      { topk_hist_kernel<0><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift); count_launches(1); }
     else
-      topk_hist_kernel<1><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift);
-    topk_pick_kernel<<<1, 256, 0, stream>>>(ctl, shift);
+      { topk_hist_kernel<1><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift); count_launches(1); }
+    { topk_pick_kernel<<<1, 256, 0, stream>>>(ctl, shift); count_launches(1); }
   }
-  if (key_type == 0) topk_count_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce);
-  else topk_count_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce);
-  scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cg, tiles, nullptr);
-  scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(ce, tiles, nullptr);
-  if (key_type == 0) topk_scatter_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx);
-  else topk_scatter_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx);
+  if (key_type == 0) { topk_count_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce); count_launches(1); }
+  else { topk_count_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cg, tiles, nullptr); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(ce, tiles, nullptr); count_launches(1); }
+  if (key_type == 0) { topk_scatter_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx); count_launches(1); }
+  else { topk_scatter_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+// ------------------------------------------------------------ hit windows
+extern "C" int sseqs_gather_windows(const uint8_t* ascii, const int64_t* offsets,
+                                    const int32_t* lengths, const int32_t* idx, int64_t n,
+                                    int width, uint8_t* out, int32_t* out_len,
+                                    cudaStream_t stream) {
+  if (n < 0 || width < 0) return SSEQS_ERR_ARG;
+  if (n == 0 || width == 0) return SSEQS_OK;
+  if (!ascii || !offsets || !lengths || !idx || !out || !out_len) return SSEQS_ERR_ARG;
+  const int grid = (int)std::min<int64_t>(n, (int64_t)device_sm_count() * 16);
+  { gather_windows_kernel<<<grid, 128, 0, stream>>>(ascii, offsets, lengths, idx, n, width, out,
+                                                  out_len); count_launches(1); }
   return status_of(cudaGetLastError());
 }

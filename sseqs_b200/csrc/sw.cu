@@ -427,7 +427,7 @@ int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
   const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
   const int64_t need = (a.n + k.groups_per_block - 1) / k.groups_per_block;
   const int grid = (int)std::max<int64_t>(1, std::min(full, need));
-  k.fn<<<grid, kThreads, k.smem, stream>>>(a);
+  { k.fn<<<grid, kThreads, k.smem, stream>>>(a); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -438,7 +438,7 @@ int run(bool aff, SwArgs a, cudaStream_t stream) {
   if (a.Lq > kMaxQuery) return SSEQS_ERR_UNSUPPORTED;
   if (a.Lq == 0) {   // sseqs/sw.cu:73: every result is -1
     const int grid = (int)std::min<int64_t>((a.n + 255) / 256, 4096);
-    fill_kernel<<<grid, 256, 0, stream>>>(a.out, a.n, -1);
+    { fill_kernel<<<grid, 256, 0, stream>>>(a.out, a.n, -1); count_launches(1); }
     return status_of(cudaGetLastError());
   }
   if (!a.q) return SSEQS_ERR_ARG;
@@ -450,7 +450,7 @@ int run(bool aff, SwArgs a, cudaStream_t stream) {
   }
   if (a.skip != 0) return SSEQS_ERR_UNSUPPORTED;
   const int grid = (int)std::min<int64_t>((a.n + 127) / 128, (int64_t)device_sm_count() * 4);
-  sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0);
+  { sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -514,9 +514,9 @@ extern "C" int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return SSEQS_ERR_CUDA;
   if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return SSEQS_ERR_CUDA; }
-  dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters / 8, 0x12345u);   // warm-up
+  { dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters / 8, 0x12345u); count_launches(1); }   // warm-up
   cudaEventRecord(e0, stream);
-  dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters, 0x12345u);
+  { dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters, 0x12345u); count_launches(1); }
   cudaEventRecord(e1, stream);
   cudaError_t err = cudaEventSynchronize(e1);
   float ms = 0.f;

@@ -206,6 +206,6 @@ extern "C" int sseqs_backtrack_affine(const uint8_t* query, int query_len, const
   TbArgs a{query, query_len, tbytes, toff, tlen, B, gap_open, gap_extend, dir, ds,
            top, top_ints(max_target_len), best, info, q_aligned, t_aligned, cap, m_full, tcols,
            max_target_len};
-  traceback_kernel<<<B, 32, 0, stream>>>(a);
+  { traceback_kernel<<<B, 32, 0, stream>>>(a); count_launches(1); }
   return status_of(cudaGetLastError());
 }

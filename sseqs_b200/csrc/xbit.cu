@@ -104,9 +104,9 @@ extern "C" int sseqs_xbit_decompress(const uint8_t* packed, uint8_t* out, int64_
   const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)device_sm_count() * 8);
   const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
   if (aligned)
-    xbit_decode_kernel<true><<<grid, kDecThreads, 0, stream>>>(packed + lo_bytes, out, n_syms);
+    { xbit_decode_kernel<true><<<grid, kDecThreads, 0, stream>>>(packed + lo_bytes, out, n_syms); count_launches(1); }
   else
-    xbit_decode_kernel<false><<<grid, kDecThreads, 0, stream>>>(packed + lo_bytes, out, n_syms);
+    { xbit_decode_kernel<false><<<grid, kDecThreads, 0, stream>>>(packed + lo_bytes, out, n_syms); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -117,6 +117,6 @@ extern "C" int sseqs_xbit_compress(const uint8_t* in, uint8_t* out, int64_t n_sy
   if (!in || !out) return SSEQS_ERR_ARG;
   const int64_t n_groups = (n_syms + 7) / 8;
   const int grid = (int)std::min<int64_t>((n_groups + 255) / 256, (int64_t)device_sm_count() * 16);
-  xbit_encode_kernel<<<grid, 256, 0, stream>>>(in, out, n_syms);
+  { xbit_encode_kernel<<<grid, 256, 0, stream>>>(in, out, n_syms); count_launches(1); }
   return status_of(cudaGetLastError());
 }

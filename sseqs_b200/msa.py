@@ -1,0 +1,224 @@
+"""``msa(queries, filenames, ...)`` -- database search and a3m output.
+
+Same signature, defaults and output files as sseqs/msa.py:71-446.  Per query
+and per database batch the stages of sseqs/msa.py:227-370 run on the GPU
+against the HBM-resident database:
+
+  prefilter (skipped when ``top_fft == 1``: every segment passes)
+  -> top-k (#segments // top_fft) -> drop the lowest and highest index
+  -> linear SW, gap -1 -> top-k (// top_sw) -> affine SW, 11/1
+  -> top-k (top_sw_affine) -> score / sqrt(len(query) * longest segment)
+  -> hit strings (first 500 residues)
+
+then the hits of all batches are ranked and the best ``num_msas`` go through
+the CUDA traceback into the a3m file (sseqs/msa.py:411-437).
+
+Where the reference leaves an order unspecified (ties inside torch.topk and
+numpy's argsort), hits are ordered by score, then by database position.
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib
+import math
+import os
+import pickle
+import threading
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import select
+from ._lib import check, lib, ptr, stream_ptr, to_host
+from .database import Database, default_database
+from .to_a3m import to_a3m
+
+_sw = importlib.import_module("sseqs_b200.sw")
+
+HIT_WIDTH = 500           # sseqs/msa.py:183
+
+
+@dataclass
+class BatchHits:
+    batch: int
+    g: torch.Tensor          # filtered segment index of each hit (device, increasing)
+    affine: torch.Tensor
+    linear: torch.Tensor
+    hits: torch.Tensor       # [n, HIT_WIDTH] bytes
+    hit_len: torch.Tensor
+    maxlen: int
+    cells_linear: int
+    cells_affine: int
+
+
+class SearchStats:
+    def __init__(self):
+        self.cells = 0
+        self.stage = {}
+
+    def add(self, key, dt):
+        self.stage[key] = self.stage.get(key, 0.0) + dt
+
+
+def _gather_hits(batch, g, n):
+    out = torch.empty((max(n, 1), HIT_WIDTH), dtype=torch.uint8, device=batch.ascii.device)
+    ln = torch.empty(max(n, 1), dtype=torch.int32, device=batch.ascii.device)
+    check(lib().sseqs_gather_windows(ptr(batch.ascii), ptr(batch.offsets), ptr(batch.lengths),
+                                     ptr(g), n, HIT_WIDTH, ptr(out), ptr(ln), stream_ptr()),
+          "gather_windows")
+    return out[:n], ln[:n]
+
+
+def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200, top_sw=10,
+                 top_sw_affine=2, fft_rank=4, luts=None, stats: SearchStats | None = None,
+                 timer=None):
+    """One query against one resident batch (sseqs/msa.py:235-370)."""
+    nseg = batch.n_segments
+    dev = batch.ascii.device
+    k1 = nseg // top_fft
+    n_c = k1 - 2                                            # [1:-1] (msa.py:307)
+    if n_c <= 0:
+        return None
+    if top_fft == 1:
+        cand = None                                         # segments 1 .. nseg-2
+    else:
+        from . import conv
+        scores = conv.prefilter_batch(query, batch, luts, fft_rank)
+        cand = select.topk_indices(scores, k1)[1:-1]
+    Lq = q_enc.numel()
+    if cand is None:
+        lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, g0=1, n_targets=n_c,
+                          skip=0, gap_a=-1)
+    else:
+        lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, good_idx=cand,
+                          skip=0, gap_a=-1)
+    k2 = n_c // top_sw
+    if k2 <= 0:
+        return None
+    if top_sw == 1:
+        p2, cand2 = None, cand
+    else:
+        p2 = select.topk_indices(lin, k2)
+        cand2 = (p2 + 1) if cand is None else cand[p2.long()]
+    if timer is not None:
+        timer("affine", True)
+    if cand2 is None:
+        aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, g0=1, n_targets=k2,
+                          skip=1, gap_a=11, gap_b=1)
+    else:
+        aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, good_idx=cand2,
+                          skip=1, gap_a=11, gap_b=1)
+    if timer is not None:
+        timer("affine", False)
+    # torch.topk raises when top_sw_affine exceeds the list (msa.py:335);
+    # here the list is kept whole instead.
+    k3 = min(top_sw_affine, k2)
+    p3 = select.topk_indices(aff, k3).long()
+    if cand2 is None:
+        g = (p3 + 1).to(torch.int32)
+    else:
+        g = cand2[p3].to(torch.int32)
+    lin_s = lin[p3] if p2 is None else lin[p2.long()[p3]]
+    hits, hlen = _gather_hits(batch, g, k3)
+    return BatchHits(bi, g, aff[p3], lin_s, hits, hlen, batch.maxlen, 0, 0)
+
+
+def _norm(aff: np.ndarray, Lq: int, maxlen: int) -> np.ndarray:
+    """int32 score / sqrt(len(query) * maxlen) in float32 (msa.py:345)."""
+    return (aff.astype(np.float32) / np.sqrt(np.float32(Lq * maxlen))).astype(np.float32)
+
+
+def rank_hits(query: str, per_batch: list, num_msas: int):
+    """Concatenate batch hits, order by normalised score (desc), then batch
+    and segment position (asc); keep ``num_msas`` (msa.py:411-427)."""
+    rows = []
+    for bh in per_batch:
+        if bh is None:
+            continue
+        g, aff, lin = to_host(bh.g), to_host(bh.affine), to_host(bh.linear)
+        hb, hl = to_host(bh.hits), to_host(bh.hit_len)
+        norm = _norm(aff, len(query), bh.maxlen)
+        for r in range(g.size):
+            rows.append((float(norm[r]), bh.batch, int(g[r]), int(aff[r]), int(lin[r]),
+                         hb[r, :hl[r]].tobytes().decode("latin-1")))
+    rows.sort(key=lambda x: (-x[0], x[1], x[2]))
+    return rows[:num_msas]
+
+
+def search(queries, db: Database | None = None, *, num_msas=4096, top_fft=200, top_sw=10,
+           top_sw_affine=2, fft_rank=4, dlength=1e6, stats: SearchStats | None = None,
+           timer=None, bs: int | None = None):
+    """Ranked hits of every query: list (per query) of tuples
+    (normalised score, batch, segment, affine, linear, hit string)."""
+    if isinstance(queries, str):
+        queries = [queries]
+    db = default_database(bs) if db is None else db
+    from . import conv
+    out = []
+    for query in queries:
+        q_enc = _sw.encode_query(query, device=db.device)
+        luts = conv.prefilter_luts(query, fft_rank) if top_fft != 1 else None
+        per = []
+        for bi, batch in enumerate(db.batches):
+            if abs(len(query) - batch.maxlen) > dlength:   # msa.py:252
+                continue
+            t0 = time.time()
+            per.append(search_batch(q_enc, query, batch, bi, top_fft=top_fft, top_sw=top_sw,
+                                    top_sw_affine=top_sw_affine, fft_rank=fft_rank, luts=luts,
+                                    stats=stats, timer=timer))
+            if stats is not None:
+                stats.add("t_sw", time.time() - t0)
+        out.append(rank_hits(query, per, num_msas))
+    return out
+
+
+def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50_000_000,
+        fft_rank=4, top_fft=200, top_sw=10, top_sw_affine=2, return_timings=False,
+        sync_time=False, dlength=1e6, gpu: int = 0, blocking: bool = True, db=None):
+    """Search every query and write one a3m file per query (sseqs/msa.py:71-446).
+
+    ``bs`` is the batch size the database was decoded with (a resident
+    ``Database`` fixes it at load time); ``db`` selects a database other than
+    the DBPATH/CHUNKS default.  ``blocking=False`` runs in a thread and
+    returns it, as the reference does.
+    """
+    if not blocking:
+        t = threading.Thread(target=msa, args=(queries, filenames, num_msas, save_raw, verbose,
+                                               bs, fft_rank, top_fft, top_sw, top_sw_affine,
+                                               return_timings, sync_time, dlength, gpu, True, db))
+        t.start()
+        return t
+    with torch.cuda.device(gpu):
+        if isinstance(queries, str):
+            queries = [queries]
+        if isinstance(filenames, str):
+            filenames = [filenames]
+        if filenames is None:
+            filenames = [hashlib.sha256(q.encode()).hexdigest()[:8] + ".a3m" for q in queries]
+        for f in filenames:
+            if f is not None and os.path.exists(f):
+                os.remove(f)
+        stats = SearchStats()
+        t0 = time.time()
+        ranked = search(queries, db, num_msas=num_msas, top_fft=top_fft, top_sw=top_sw,
+                        top_sw_affine=top_sw_affine, fft_rank=fft_rank, dlength=dlength,
+                        stats=stats, bs=bs)
+        if sync_time:
+            torch.cuda.synchronize()
+        stats.add("t_search", time.time() - t0)
+        for query, fname, rows in zip(queries, filenames, ranked):
+            if save_raw != "":
+                pickle.dump([query, [r[5] for r in rows], [r[4] for r in rows], [],
+                             [r[0] for r in rows]], open(save_raw, "wb"))
+            t1 = time.time()
+            if fname is not None:
+                if verbose:
+                    print(f"Saving result to {fname}")
+                to_a3m(query, [r[5] for r in rows], fname)
+            stats.add("t_a3m", time.time() - t1)
+        if verbose:
+            print(f"searched {len(queries)} queries, {sum(len(r) for r in ranked)} hits")
+        if return_timings:
+            return dict(stats.stage)

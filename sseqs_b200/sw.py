@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._lib import check, lib, ptr, require_cuda, stream_ptr, workspace
+from ._lib import check, lib, ptr, require_cuda, stream_ptr, to_device, to_host, workspace
 
 AA = "ARNDCQEGHILKMFPSTWYV"
 AA_MAP = {aa: i for i, aa in enumerate(AA)}
@@ -90,7 +90,8 @@ def sw_scan(query_idx: torch.Tensor, ascii: torch.Tensor, delim: torch.Tensor, *
 
 def encode_query(query: str, device="cuda") -> torch.Tensor:
     """Class indices of the standard residues of ``query`` (sseqs/sw.py:11)."""
-    return torch.tensor([AA_MAP[c] for c in query if c in AA_MAP], dtype=torch.uint8, device=device)
+    return to_device(torch.tensor([AA_MAP[c] for c in query if c in AA_MAP], dtype=torch.uint8),
+                     device)
 
 
 def sw(query: str, targets: list[str], gap_open: int = 11, gap_extend: int = 1) -> torch.Tensor:
@@ -117,10 +118,8 @@ class Alignments:
         self.cap, self.m_full = cap, m_full
 
     def to_dicts(self) -> list[dict]:
-        best = self.best.cpu().numpy()
-        info = self.info.cpu().numpy()
-        q_al = self.q_al.cpu().numpy()
-        t_al = self.t_al.cpu().numpy()
+        best, info = to_host(self.best), to_host(self.info)
+        q_al, t_al = to_host(self.q_al), to_host(self.t_al)
         out = []
         for b in range(best.shape[0]):
             n = int(info[b, 0])
@@ -158,10 +157,10 @@ def backtrack(query: str, targets: list[str], gap_open: int = 11, gap_extend: in
         toff_h[1:] = np.cumsum(tlen_h[:-1])
     blob = b"".join(tbs)
     dev = torch.device(device)
-    tbytes = torch.from_numpy(np.frombuffer(blob + b"\0" * 16, dtype=np.uint8).copy()).to(dev)
-    toff = torch.from_numpy(toff_h).to(dev)
-    tlen = torch.from_numpy(tlen_h).to(dev)
-    q = torch.from_numpy(np.frombuffer(qb + b"\0", dtype=np.uint8).copy()).to(dev)
+    tbytes = to_device(torch.from_numpy(np.frombuffer(blob + b"\0" * 16, dtype=np.uint8).copy()), dev)
+    toff = to_device(torch.from_numpy(toff_h), dev)
+    tlen = to_device(torch.from_numpy(tlen_h), dev)
+    q = to_device(torch.from_numpy(np.frombuffer(qb + b"\0", dtype=np.uint8).copy()), dev)
     cap = len(qb) + tmax + 1
     best = torch.zeros(B, dtype=torch.int32, device=dev)
     info = torch.empty((B, 5), dtype=torch.int32, device=dev)

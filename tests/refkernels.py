@@ -66,3 +66,37 @@ def decompress(packed, n, lo):
     lib().decompress_launcher(packed.data_ptr(), out.data_ptr(), n, lo)
     torch.cuda.synchronize()
     return out[:n]
+
+
+def warp_corr(query: str, A, B, ascii, offsets, lengths, n, k):
+    """The reference prefilter (sseqs/filter.cu:161-395) on a batch.
+
+    Two over-reads of the reference are given memory to land in: the query
+    spectrum scratch holds k*(n+2) halves (the kernel writes k*(n/2+1)
+    half2), and the database table holds at least 100 floats (the kernel
+    stages W_db[0..99], sseqs/fft.cu:91-93), zero past the k x 21 table.
+    """
+    import numpy as np
+    import torch
+    AA = "ARNDCQEGHILKMFPSTWYV"
+    pos = {a: i for i, a in enumerate(AA)}
+    pos.update({"X": 20, "-": 20, "*": 20})
+    qrev = torch.tensor([pos.get(c, 20) for c in query[::-1]], dtype=torch.uint8, device="cuda")
+    Ad = torch.from_numpy(np.ascontiguousarray(A[:k], np.float32)).cuda()
+    Bpad = np.zeros(max(100, (k + 1) * 21), np.float32)
+    Bpad[:k * 21] = np.asarray(B[:k], np.float32).reshape(-1)
+    Bd = torch.from_numpy(Bpad).cuda()
+    nseg = lengths.numel()
+    corr = torch.zeros(nseg, dtype=torch.float16, device="cuda")
+    stats = torch.empty((nseg, 2), dtype=torch.float32, device="cuda")
+    scratch = torch.zeros(k * (n + 2) + 64, dtype=torch.float16, device="cuda")
+    off32 = offsets.to(torch.int32).contiguous()
+    ln32 = lengths.to(torch.int32).contiguous()
+    maxlen = int(ln32.max().item())
+    torch.cuda.synchronize()
+    lib().launch_warp_corr(corr.data_ptr(), qrev.data_ptr(), Ad.data_ptr(), Bd.data_ptr(),
+                           ascii.data_ptr(), off32.data_ptr(), ln32.data_ptr(), stats.data_ptr(),
+                           nseg, 21, k, len(query), maxlen, n,
+                           torch.cuda.current_stream().cuda_stream, scratch.data_ptr())
+    torch.cuda.synchronize()
+    return corr

@@ -1,0 +1,128 @@
+"""GPU tests of the search pipeline: prefilter (tolerance), and the whole
+per-batch search and a3m output against the CPU oracle (exact)."""
+import importlib
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests import refkernels
+
+pytestmark = pytest.mark.gpu
+
+
+def _db(n_seqs=4000, chunk_bytes=150_000, Lq=180, seed=0, frac=0.02):
+    from sseqs_b200 import dbtools
+    q = dbtools.random_query(Lq, seed)
+    syn = dbtools.synthetic_db([q], n_seqs, frac, (0.3, 0.9), seed=seed, device="cpu",
+                               chunk_bytes=chunk_bytes)
+    return q, syn
+
+
+def _host_batches(syn, bs):
+    """Decoded batches exactly as sseqs/msa.py:217-220 slices the chunks."""
+    out = []
+    for c in syn.chunks:
+        c = c.numpy()
+        for j in range(c.size // bs):
+            out.append(O.xbit_decompress(c, int(bs * 8 / 5), j * bs))
+    return out
+
+
+@pytest.mark.parametrize("Lq,maxlen_cap", [(180, None), (600, None), (40, 50)])
+def test_prefilter_matches_float64_oracle(Lq, maxlen_cap):
+    from sseqs_b200 import conv, select, dbtools
+    rng = np.random.default_rng(Lq)
+    query = dbtools.random_query(Lq, Lq)
+    lens = rng.integers(5, maxlen_cap or 1000, 700)
+    segs = [dbtools.random_query(int(n), 100 + i) for i, n in enumerate(lens)]
+    segs[3] = segs[3][:10] + "XXXBZ" + segs[3][10:]
+    ascii = np.frombuffer(("@".join(segs) + "@").encode(), np.uint8).copy()
+    seg = O.segment(ascii)
+    n = conv.transform_length(Lq, int(seg["lengths"].max()))
+    A, B = O.prefilter_luts(query, 4)
+    exp = O.prefilter_scores(query, A, B, ascii, seg["offsets"], seg["lengths"], n, 4)
+    luts = conv.prefilter_luts(query, 4)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    got = conv.prefilter_scores(luts, d(ascii), d(seg["offsets"]), d(seg["lengths"].astype(np.int32)),
+                                len(seg["lengths"]), n, 4).float().cpu().numpy()
+    tol = 2e-3 * np.maximum(1.0, np.abs(exp))
+    assert np.all(np.abs(got - exp) <= tol), np.max(np.abs(got - exp) / np.maximum(1, np.abs(exp)))
+    if refkernels.available() and n <= 1024:
+        ref = refkernels.warp_corr(query, A, B, d(ascii), d(seg["offsets"]),
+                                   d(seg["lengths"]), n, 4).float().cpu().numpy()
+        # the reference computes in fp16: compare loosely, and compare the
+        # candidate sets a top-1/10 selection takes
+        assert np.corrcoef(ref, exp)[0, 1] > 0.99
+        k = len(exp) // 10
+        a = set(np.argsort(-ref, kind="stable")[:k])
+        b = set(np.argsort(-got, kind="stable")[:k])
+        assert len(a & b) >= 0.9 * k
+
+
+def _oracle_search(query, batches, prefilter_fn=None, **kw):
+    """Oracle restatement over the non-empty batches (numbered in order)."""
+    rows = []
+    bi = 0
+    for a in batches:
+        seg = O.segment(a)
+        if seg["lengths"].size == 0:
+            continue
+        scores = prefilter_fn(bi) if prefilter_fn else None
+        for g, aff, lin, norm, s in O.search_batch(query, a, prefilter=scores, **kw):
+            rows.append((norm, bi, g, aff, lin, s))
+        bi += 1
+    rows.sort(key=lambda x: (-x[0], x[1], x[2]))
+    return rows
+
+
+@pytest.mark.parametrize("top_sw,top_sw_affine", [(1, 60), (3, 25)])
+def test_exact_search_matches_oracle(top_sw, top_sw_affine):
+    from sseqs_b200.database import Database
+    M = importlib.import_module("sseqs_b200.msa")
+    q, syn = _db()
+    bs = 50_000
+    db = Database(syn.chunks, bs=bs)
+    got = M.search([q], db, num_msas=10_000, top_fft=1, top_sw=top_sw,
+                   top_sw_affine=top_sw_affine)[0]
+    exp = _oracle_search(q, _host_batches(syn, bs), top_fft=1, top_sw=top_sw,
+                         top_sw_affine=top_sw_affine)
+    assert len(got) == len(exp)
+    for a, b in zip(got, exp):
+        assert a[1:] == b[1:]
+        assert a[0] == pytest.approx(b[0], rel=0, abs=0)
+
+
+def test_prefiltered_search_matches_oracle_given_scores():
+    from sseqs_b200 import conv
+    from sseqs_b200.database import Database
+    M = importlib.import_module("sseqs_b200.msa")
+    q, syn = _db(seed=3)
+    bs = 75_000
+    db = Database(syn.chunks, bs=bs)
+    got = M.search([q], db, num_msas=10_000, top_fft=7, top_sw=2, top_sw_affine=10)[0]
+    luts = conv.prefilter_luts(q, 4)
+    batches = _host_batches(syn, bs)
+    scores = [conv.prefilter_batch(q, b, luts, 4).float().cpu().numpy() for b in db.batches]
+    assert sum(1 for b in batches if O.segment(b)["lengths"].size) == len(scores)
+    exp = _oracle_search(q, batches, top_fft=7, top_sw=2, top_sw_affine=10,
+                         prefilter_fn=lambda bi: scores[bi])
+    assert [r[1:] for r in got] == [r[1:] for r in exp]
+
+
+def test_msa_writes_oracle_a3m(tmp_path):
+    from sseqs_b200.database import Database
+    import sseqs_b200
+    q, syn = _db(n_seqs=3000, seed=5)
+    db = Database(syn.chunks, bs=150_000)
+    f = tmp_path / "out.a3m"
+    sseqs_b200.msa(q, str(f), num_msas=200, top_fft=1, top_sw=1, top_sw_affine=200, bs=150_000,
+                   db=db, verbose=False)
+    rows = _oracle_search(q, _host_batches(syn, 150_000), top_fft=1, top_sw=1,
+                          top_sw_affine=200)[:200]
+    _, al = O.sw_affine_backtrack(q, [r[5] for r in rows])
+    assert f.read_text() == O.to_a3m_text(q, al)
+    # planted homologs dominate the top of the list
+    assert sum(1 for r in rows[:20] if r[3] > 100) >= 15

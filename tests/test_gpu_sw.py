@@ -1,5 +1,6 @@
 """GPU parity of the score kernels: CUDA vs the CPU oracle vs the reference's
 own CUDA kernels, bit-exact (int32 scores)."""
+import importlib
 import os
 
 import numpy as np
@@ -34,7 +35,7 @@ QUERY_LENGTHS = [1, 2, 17, 32, 33, 64, 65, 100, 128, 129, 200, 256, 257, 300, 50
 
 @pytest.mark.parametrize("Lq", QUERY_LENGTHS)
 def test_sw_ops_match_oracle(Lq):
-    from sseqs_b200 import sw as S
+    S = importlib.import_module("sseqs_b200.sw")
     n = 600 if Lq <= 300 else (250 if Lq <= 1024 else 120)
     query, q, ascii, starts = _case(Lq, Lq, n, extra="XBZU*@")
     good = np.arange(len(starts), dtype=np.int32)
@@ -56,7 +57,7 @@ def test_sw_ops_match_oracle(Lq):
 def test_sw_ops_match_reference_cuda_kernels(Lq):
     if not refkernels.available():
         pytest.skip("oracle/_ref/libsseqs_ref.so not built")
-    from sseqs_b200 import sw as S
+    S = importlib.import_module("sseqs_b200.sw")
     query, q, ascii, starts = _case(1000 + Lq, Lq, 700, extra="XB")
     good = np.arange(1, len(starts), dtype=np.int32)     # g >= 1: defined windows
     qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
@@ -75,7 +76,7 @@ def test_sw_ops_match_reference_cuda_kernels(Lq):
 
 def test_scan_matches_reference_windows():
     """sw_scan over a decoded batch == the two window forms msa() uses."""
-    from sseqs_b200 import sw as S
+    S = importlib.import_module("sseqs_b200.sw")
     query, q, ascii, starts = _case(77, 333, 3000)
     pad = np.full(100, 64, np.uint8)             # '@' padding as in a packed chunk
     ascii = np.concatenate([ascii, pad])
@@ -99,7 +100,7 @@ def test_scan_matches_reference_windows():
 
 
 def test_nonstandard_gap_parameters_use_exact_generic_path():
-    from sseqs_b200 import sw as S
+    S = importlib.import_module("sseqs_b200.sw")
     query, q, ascii, starts = _case(5, 90, 200)
     good = np.arange(len(starts), dtype=np.int32)
     qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
@@ -110,7 +111,7 @@ def test_nonstandard_gap_parameters_use_exact_generic_path():
 
 
 def test_degenerate_inputs():
-    from sseqs_b200 import sw as S
+    S = importlib.import_module("sseqs_b200.sw")
     q = _dev(O.encode_query("MKTAYIAKQRQ"))
     ascii = _dev(np.frombuffer(b"MKTAYIAK@@QRQ@W@", np.uint8).copy())
     starts = np.array([8, 9, 13, 15, 15, 3], np.int32)
