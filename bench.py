@@ -135,12 +135,17 @@ def segment_cells(db):
     return tot
 
 
-def run_step(M, query, db, timer=None):
-    """Device part of one step: search, rank, traceback (no file I/O)."""
-    from sseqs_b200.to_a3m import a3m_text, align_all
+def run_step(M, query, db, timer=None, world=1, rank=0):
+    """Device part of one step: search, rank, traceback (no file I/O).  With
+    several GPUs every rank searches its own shard, the ranked hits are merged
+    across ranks, and rank 0 aligns the merged list."""
+    from sseqs_b200.to_a3m import align_all
     rows = M.search([query], db, num_msas=TOP_K, top_fft=1, top_sw=1, top_sw_affine=TOP_K,
                     timer=timer)[0]
-    al = align_all(query, [r[5] for r in rows])
+    if world > 1:
+        from sseqs_b200 import shard
+        rows = [r[:1] + r[2:] for r in shard.gather_hits(rows, TOP_K)]
+    al = align_all(query, [r[5] for r in rows]) if rank == 0 else None
     return rows, al
 
 
@@ -208,7 +213,7 @@ def bench_b200(args):
     res_cells = segment_cells(db)
     warm, timed = step_queries(queries, args.steps, args.warmup)
     for q in warm:
-        run_step(M, q, db)
+        run_step(M, q, db, world=world, rank=rank)
     torch.cuda.synchronize()
 
     aff_events = []
@@ -234,7 +239,7 @@ def bench_b200(args):
     e0.record()
     cells = 0
     for q in timed:
-        run_step(M, q, db, timer=timer)
+        run_step(M, q, db, timer=timer, world=world, rank=rank)
         cells += 2 * len(q) * res_cells
     e1.record()
     torch.cuda.synchronize()

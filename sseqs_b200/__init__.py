@@ -1,15 +1,12 @@
 """sseqs_b200 -- the sseqs database-search path on NVIDIA B200 (sm_100a).
 
-Drop-in for the reference's public calls: ``msa(query, "out.a3m")`` and
-``sw(query, targets)``; ``sseqs_b200.sw`` also holds ``sw_affine_backtrack``
-and the extension operators ``sw_cuda_blosum62`` / ``sw_cuda_affine``,
-``sseqs_b200.xbit`` the codec and ``sseqs_b200.to_a3m`` the a3m writer.
+Drop-in for the reference's public calls (sseqs/__init__.py:1-2):
+``msa(query, "out.a3m")`` and ``sw(query, targets)``.  As in the reference,
+the package attributes ``msa`` and ``sw`` are the functions; the modules
+``sseqs_b200.sw`` (``sw_affine_backtrack``, ``sw_cuda_blosum62``,
+``sw_cuda_affine``), ``sseqs_b200.xbit``, ``sseqs_b200.conv`` and
+``sseqs_b200.to_a3m`` hold the rest.
 """
+from .msa import msa  # noqa: F401
 from .sw import sw  # noqa: F401
-
-
-def __getattr__(name):
-    if name in ("msa", "Database"):
-        from . import msa as _m
-        return getattr(_m, name)
-    raise AttributeError(name)
+from .database import Database  # noqa: F401

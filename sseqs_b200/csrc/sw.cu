@@ -9,25 +9,35 @@
 // any lane mapping.
 //
 // B200 mapping.  Two stripes of the same target share one 32-bit register as
-// int16x2 (lo = stripe 2m, hi = stripe 2m+1) and advance together through
-// the DPX instructions (__viaddmax_s16x2_relu, __vimax3_s16x2, ...).  A lane
-// holds W such words per column, so a target occupies G = 32/(2W) lanes and
-// a warp scores 2W targets side by side.  The query profile (score of each
-// residue class against every column, already packed as the lane's int16x2
-// words) sits in shared memory; a lane fetches its row of it with 128-bit
-// loads.  Per word-column the recurrences cost
-//   linear: max(up, left); diag + s; max(. + gap, ., 0)       -> 3 ops
-//   affine: M = max(diag + s, 0); M - open; Ix chain; D = max3(M, Ix, Iy);
-//           next-row Iy = max(Iy - ext, M - open, 0)          -> 5 ops
-// plus half a max3 for the running best.  All cell values are >= 0 and at
-// most 11 * Lq <= 22528, so int16 lanes cannot overflow for Lq <= 2048 (no
-// int32 re-run is ever needed).
+// int16x2 (lo = stripe 2m, hi = stripe 2m+1).  A lane holds W such words per
+// column, so a target occupies G = 32/(2W) lanes and a warp scores 2W
+// targets side by side.  The query profile (score of each residue class
+// against every column, already packed as the lane's int16x2 words) sits in
+// shared memory; a lane fetches its row of it with 128-bit loads.
 //
-// Targets are streamed: each lane group walks a contiguous range of targets,
-// reading the target bytes through 16-byte chunk loads with one chunk of
-// look-ahead, and when a target ends the group writes its score, resets its
-// state and moves on while the other groups of the warp keep going (idle
-// groups score a padding class that never raises a score).
+// Every int16x2 instruction used here issues at half rate on its pipe: the
+// max-type DPX instructions (__vimax3_s16x2_relu, __viaddmax_s16x2_relu) on
+// the ALU pipe, the int16x2 add/sub (__vadd2, __vsub2) on the FMA pipe.  A
+// scheduler issues one instruction per clock, so the recurrences are written
+// to spread work over both pipes:
+//   affine, per word-column (2 cells): M' = D_diag + s, Mo = M' - open (FMA);
+//     Ix = max(Ix_left - ext, Mo_left, 0), D = max(M', Ix, Iy, 0),
+//     next-row Iy = max(Iy - ext, Mo, 0), half a running max (ALU)
+//     -> 3.5 ALU + 2 FMA;
+//   linear, with the state carried as H + gap: u = Hg_diag + (s - gap) (FMA),
+//     H = max(u, Hg_up, Hg_left, 0), half a running max (ALU),
+//     Hg = H + gap (FMA)  -> 1.5 ALU + 2 FMA.
+// M' is left unclamped: it only enters maxima that also hold 0.  All cell
+// values are >= 0 and at most 11 * Lq <= 22528, so int16 lanes cannot
+// overflow for Lq <= 2048 (no int32 re-run is ever needed); the profile's
+// padding words (-32768 + open, or -16384) keep every intermediate inside
+// int16 and can never raise a score.
+//
+// Targets are streamed: each lane group walks a contiguous range of targets
+// four rows at a time, the four bytes of the next quad prefetched with two
+// aligned 32-bit loads; when a target ends (rows past its end are padding
+// rows) the group writes its score, resets its state and moves on while the
+// other groups of the warp keep going.
 #include <algorithm>
 #include <mutex>
 
@@ -97,11 +107,6 @@ __device__ __forceinline__ int score_of(const uint8_t* q, int Lq, int cls, int j
   return qc < kNumAA ? blosum62(cls, qc) : -4;
 }
 
-__device__ __forceinline__ uint32_t byte_of(const uint4& c, int i) {
-  const uint32_t w = (i & 8) ? ((i & 4) ? c.w : c.z) : ((i & 4) ? c.y : c.x);
-  return (w >> ((i & 3) << 3)) & 0xffu;
-}
-
 template <int TPT>
 constexpr int words_for() {
   return TPT == 1 ? 16 : TPT == 2 ? 8 : TPT <= 4 ? 4 : TPT <= 8 ? 2 : 1;
@@ -126,15 +131,22 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);
   uint8_t* lut = reinterpret_cast<uint8_t*>(prof + kNumCls * L::CLS);
 
+  // Profile words.  Affine: s (real columns), -32768 + open (padding), so
+  // that M' - open never leaves int16.  Linear: s - gap (the state carries
+  // H + gap), -16384 for padding.  Padding never raises a score.
+  const int pad = AFF ? kNeg + a.p0 : -16384;
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = ascii_class((uint8_t)i);
   for (int i = threadIdx.x; i < kNumCls * L::CLS; i += blockDim.x) {
     const int c = i / L::CLS, r = i - c * L::CLS;
     const int gl = r / L::LWP, v = r - gl * L::LWP;
-    uint32_t word = pack2(kNeg, kNeg);
+    uint32_t word = pack2(pad, pad);
     if (v < L::NWD) {
       const int w = v / TPT, k = v - w * TPT;
       const int j = (gl * 2 * W + 2 * w) * TPT + k;
-      word = pack2(score_of(a.q, a.Lq, c, j), score_of(a.q, a.Lq, c, j + TPT));
+      int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + TPT);
+      s0 = (s0 == kNeg) ? pad : (AFF ? s0 : s0 - a.p0);
+      s1 = (s1 == kNeg) ? pad : (AFF ? s1 : s1 - a.p0);
+      word = pack2(s0, s1);
     }
     prof[i] = word;
   }
@@ -151,156 +163,163 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
   int64_t t = (a.n * gid) / ngroups;
   const int64_t t_hi = (a.n * (gid + 1)) / ngroups;
 
-  const uint32_t gap2 = pack2(a.p0, a.p0);    // linear gap (<= 0)
-  const uint32_t open2 = pack2(a.p0, a.p0);   // affine open (>= 0)
-  const uint32_t next2 = pack2(-a.p1, -a.p1); // affine -extend (<= 0)
+  const uint32_t gap2 = pack2(a.p0, a.p0);    // linear gap, -16384 <= gap <= 0
+  const uint32_t open2 = pack2(a.p0, a.p0);   // affine open, 0 <= open <= 16384
+  const uint32_t next2 = pack2(-a.p1, -a.p1); // affine -extend, 0 <= extend <= 16384
+  // state at row -1: H = 0 (linear state is H + gap), D = Iy = 0 (affine)
+  const uint32_t init = AFF ? 0u : gap2;
 
-  uint32_t S[W][TPT];                 // linear: H(i-1,.)  affine: D(i-1,.)
+  uint32_t S[W][TPT];                 // linear: H(i-1,.) + gap   affine: D(i-1,.)
   uint32_t Y[AFF ? W : 1][TPT];       // affine: Iy(i,.) carried into row i
   uint32_t best = 0;
+  auto reset = [&]() {
+    best = 0;
 #pragma unroll
-  for (int w = 0; w < W; ++w)
+    for (int w = 0; w < W; ++w)
 #pragma unroll
-    for (int k = 0; k < TPT; ++k) {
-      S[w][k] = 0;
-      if constexpr (AFF) Y[w][k] = 0;
+      for (int k = 0; k < TPT; ++k) {
+        S[w][k] = init;
+        if constexpr (AFF) Y[w][k] = 0;
+      }
+  };
+  reset();
+
+  // one DP row for every group of the warp (warp-uniform)
+  auto row = [&](int cls) {
+    const uint4* pr = reinterpret_cast<const uint4*>(prof + cls * L::CLS + gl * L::LWP);
+    uint32_t s[L::NV * 4];
+#pragma unroll
+    for (int v = 0; v < L::NV; ++v) {
+      const uint4 x = pr[v];
+      s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
+    uint32_t from_left = __shfl_up_sync(0xffffffffu, S[W - 1][TPT - 1], 1, G);
+    if (gl == 0) from_left = init;                  // column -1 of stripe 0
+    uint32_t din[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+      din[w] = __byte_perm(w == 0 ? from_left : S[w - 1][TPT - 1], S[w][TPT - 1], 0x5432);
+    uint32_t pend = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      uint32_t diag = din[w];
+      if constexpr (!AFF) {
+        // state Hg = H + gap:  H = max(Hg_diag + (s - gap), Hg_up, Hg_left, 0)
+        // (Hg_left = gap at the first column of a stripe)
+        uint32_t hg_left = 0;
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          const uint32_t up = S[w][k];
+          const uint32_t u = __vadd2(diag, s[w * TPT + k]);                 // FMA pipe
+          const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
+                                      : __vimax3_s16x2_relu(u, up, hg_left); // ALU pipe
+          hg_left = __vadd2(h, gap2);                                       // FMA pipe
+          diag = up;
+          S[w][k] = hg_left;
+          if (((w * TPT + k) & 1) == 0) pend = h;
+          else best = __vimax3_s16x2(best, pend, h);
+        }
+      } else {
+        // M' = D_diag + s (unclamped), Mo = M' - open          FMA pipe
+        // Ix = max(Ix_left - ext, Mo_left, 0)   (0 at k = 0)  ALU
+        // D  = max(M', Ix, Iy, 0)                             ALU
+        // Iy(next row) = max(Iy - ext, Mo, 0)                 ALU
+        uint32_t X = 0, mo_left = 0;
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          const uint32_t mp = __vadd2(diag, s[w * TPT + k]);
+          const uint32_t mo = __vsub2(mp, open2);
+          if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
+          const uint32_t y = Y[w][k];
+          const uint32_t D = (k > 0) ? __vimax3_s16x2_relu(mp, X, y) : __vimax_s16x2_relu(mp, y);
+          Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
+          diag = S[w][k];
+          S[w][k] = D;
+          mo_left = mo;
+          if (((w * TPT + k) & 1) == 0) pend = D;
+          else best = __vimax3_s16x2(best, pend, D);
+        }
+      }
+    }
+    if ((L::NWD & 1) != 0) best = __vimax_s16x2_relu(best, pend);
+  };
+
+  // ---- target bytes: four rows at a time from two aligned 32-bit words.
+  // A word is loaded only when it holds a byte of the window being read, so
+  // no load leaves the windows' own 4-byte words.
+  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
+  const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
+  const int64_t aoff = (int64_t)(au & 3);
+  struct Quad { uint32_t w0, w1; };
+  auto fetch = [&](int64_t p, int64_t e) -> Quad {
+    const int64_t ap = p + aoff;
+    const int64_t wi = ap >> 2;
+    Quad q;
+    q.w0 = __ldg(abase + wi);
+    q.w1 = ((wi + 1) << 2) < e + aoff ? __ldg(abase + wi + 1) : 0u;
+    return q;
+  };
+  uint32_t c0 = kClsPad, c1 = kClsPad, c2 = kClsPad, c3 = kClsPad;
+  auto classes = [&](const Quad& q, int64_t p, int64_t e) {
+    const uint32_t raw = __funnelshift_r(q.w0, q.w1, (uint32_t)((p + aoff) & 3) * 8u);
+    c0 = p + 0 < e ? lut[raw & 0xffu] : kClsPad;
+    c1 = p + 1 < e ? lut[(raw >> 8) & 0xffu] : kClsPad;
+    c2 = p + 2 < e ? lut[(raw >> 16) & 0xffu] : kClsPad;
+    c3 = p + 3 < e ? lut[raw >> 24] : kClsPad;
+  };
 
   // ---- target bookkeeping (group-uniform) ----
   Win cur, nxt;
   bool active = false, nxt_ok = false;
-  while (t < t_hi) {
-    cur = window_of(a, t);
-    if (cur.rows) { active = true; break; }
-    if (gl == 0) a.out[t] = cur.res;
-    ++t;
-  }
-  if (active && t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
-
-  // ---- byte stream: 16-byte chunks relative to an aligned base ----
-  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
-  const uint4* abase = reinterpret_cast<const uint4*>(au & ~(uintptr_t)15);
-  const int64_t aoff = (int64_t)(au & 15);
-  int64_t cid = -2;
-  uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
-  bool c1ok = false;
-  // A chunk is loaded only when it holds a byte that will be scored, so no
-  // load can touch memory outside the windows' 16-byte chunks.
-  auto used = [&](int64_t c) -> bool {
-    return (c << 4) < cur.end + aoff ||
-           (nxt_ok && nxt.rows && c == ((nxt.pos + aoff) >> 4));
-  };
-  auto seek = [&]() {
-    const int64_t c = (cur.pos + aoff) >> 4;
-    if (c != cid) {
-      if (c == cid + 1 && c1ok) {
-        c0 = c1;
-      } else {
-        c0 = __ldg(abase + c);
-      }
-      cid = c;
-      c1ok = false;
+  auto start_from = [&](int64_t tt) {   // first target at or after tt with rows
+    active = false;
+    nxt_ok = false;
+    t = tt;
+    while (t < t_hi) {
+      cur = window_of(a, t);
+      if (cur.rows) { active = true; break; }
+      if (gl == 0) a.out[t] = cur.res;
+      ++t;
     }
-    if (!c1ok && used(cid + 1)) {
-      c1 = __ldg(abase + cid + 1);
-      c1ok = true;
-    }
+    if (active && t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
   };
-  if (active) seek();
+  start_from(t);
+  if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
 
   while (__any_sync(0xffffffffu, active)) {
-    int cls = kClsPad;
-    if (active) cls = lut[byte_of(c0, (int)((cur.pos + aoff) & 15))];
-
-    // ---------------- one DP row for every group of the warp ----------------
-    {
-      const uint4* pr = reinterpret_cast<const uint4*>(prof + cls * L::CLS + gl * L::LWP);
-      uint32_t s[L::NV * 4];
-#pragma unroll
-      for (int v = 0; v < L::NV; ++v) {
-        const uint4 x = pr[v];
-        s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
-      }
-      uint32_t from_left = __shfl_up_sync(0xffffffffu, S[W - 1][TPT - 1], 1, G);
-      if (gl == 0) from_left = 0;
-      uint32_t din[W];
-#pragma unroll
-      for (int w = 0; w < W; ++w)
-        din[w] = __byte_perm(w == 0 ? from_left : S[w - 1][TPT - 1], S[w][TPT - 1], 0x5432);
-
-      uint32_t pend = 0;
-#pragma unroll
-      for (int w = 0; w < W; ++w) {
-        uint32_t diag = din[w];
-        if constexpr (!AFF) {
-          uint32_t left = 0;
-#pragma unroll
-          for (int k = 0; k < TPT; ++k) {
-            const uint32_t up = S[w][k];
-            const uint32_t m = (k == 0) ? up : __vmaxs2(up, left);
-            const uint32_t u = __vadd2(diag, s[w * TPT + k]);
-            const uint32_t h = __viaddmax_s16x2_relu(m, gap2, u);
-            diag = up;
-            S[w][k] = h;
-            left = h;
-            if (((w * TPT + k) & 1) == 0) pend = h;
-            else best = __vimax3_s16x2(best, pend, h);
-          }
-        } else {
-          uint32_t X = 0, mo_left = 0;
-#pragma unroll
-          for (int k = 0; k < TPT; ++k) {
-            const uint32_t M = __viaddmax_s16x2_relu(diag, s[w * TPT + k], 0u);
-            const uint32_t mo = __vsub2(M, open2);
-            if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
-            const uint32_t y = Y[w][k];
-            const uint32_t D = __vimax3_s16x2(M, X, y);
-            Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
-            diag = S[w][k];
-            S[w][k] = D;
-            mo_left = mo;
-            if (((w * TPT + k) & 1) == 0) pend = D;
-            else best = __vimax3_s16x2(best, pend, D);
-          }
-        }
-      }
-      if ((L::NWD & 1) != 0) best = __vmaxs2(best, pend);
-    }
-
+    // prefetch the bytes of the next quad of this group
+    Quad pf{0u, 0u};
+    bool pf_nxt = false;
     if (active) {
-      ++cur.pos;
-      if (cur.pos == cur.end) {
-        // target finished: reduce the group's best, reset, move on
+      if (cur.pos + 4 < cur.end) pf = fetch(cur.pos + 4, cur.end);
+      else if (nxt_ok && nxt.rows) { pf = fetch(nxt.pos, nxt.end); pf_nxt = true; }
+    }
+    row(c0);
+    row(c1);
+    row(c2);
+    row(c3);
+    if (active) {
+      cur.pos += 4;
+      if (cur.pos >= cur.end) {
+        // target finished (rows past its end were padding rows)
         int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
         if (gl == 0) a.out[t] = v;
-        best = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-#pragma unroll
-          for (int k = 0; k < TPT; ++k) {
-            S[w][k] = 0;
-            if constexpr (AFF) Y[w][k] = 0;
-          }
-        ++t;
-        active = false;
-        if (t < t_hi) {
-          cur = nxt_ok ? nxt : window_of(a, t);
+        reset();
+        if (pf_nxt) {
+          ++t;
+          cur = nxt;
           nxt_ok = false;
-          while (!cur.rows) {
-            if (gl == 0) a.out[t] = cur.res;
-            if (++t >= t_hi) break;
-            cur = window_of(a, t);
-          }
-          if (t < t_hi) {
-            active = true;
-            if (t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
-            seek();
-          }
+          if (t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
+          classes(pf, cur.pos, cur.end);
+        } else {
+          start_from(t + 1);
+          if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
+          else c0 = c1 = c2 = c3 = kClsPad;
         }
-      } else if (((cur.pos + aoff) & 15) == 0) {
-        seek();
+      } else {
+        classes(pf, cur.pos, cur.end);
       }
     }
   }
@@ -442,12 +461,11 @@ int run(bool aff, SwArgs a, cudaStream_t stream) {
     return status_of(cudaGetLastError());
   }
   if (!a.q) return SSEQS_ERR_ARG;
-  const bool fast = aff ? (a.p0 >= 0 && a.p1 >= 0) : (a.p0 <= 0);
-  if (fast) {
-    a.p0 = aff ? std::min(a.p0, 32767) : std::max(a.p0, -32768);
-    a.p1 = std::min(a.p1, 32767);
-    return launch_stream(a, aff, stream);
-  }
+  // The int16x2 kernel needs every intermediate inside int16: cells are in
+  // [0, 11*2048], profile words s - open in [-16388, 11].
+  const bool fast = aff ? (a.p0 >= 0 && a.p0 <= 16384 && a.p1 >= 0 && a.p1 <= 16384)
+                        : (a.p0 <= 0 && a.p0 >= -16384);
+  if (fast) return launch_stream(a, aff, stream);
   if (a.skip != 0) return SSEQS_ERR_UNSUPPORTED;
   const int grid = (int)std::min<int64_t>((a.n + 127) / 128, (int64_t)device_sm_count() * 4);
   { sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0); count_launches(1); }
