@@ -149,13 +149,15 @@ def run_step(M, query, db, timer=None, world=1, rank=0):
     return rows, al
 
 
-def dpx_peak():
+def measured_peak(name):
+    """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
+    int pipes), in int16x2 lane-instructions per second."""
     import torch
     from sseqs_b200 import _lib
     sink = torch.zeros(1, dtype=torch.int32, device="cuda")
     v = ctypes.c_double()
-    _lib.check(_lib.lib().sseqs_dpx_peak(sink.data_ptr(), ctypes.byref(v), _lib.stream_ptr()),
-               "dpx_peak")
+    _lib.check(getattr(_lib.lib(), name)(sink.data_ptr(), ctypes.byref(v), _lib.stream_ptr()),
+               name)
     return v.value
 
 
@@ -211,6 +213,8 @@ def bench_b200(args):
     # weak scaling: every rank holds its own database shard of DB_SEQS sequences
     db, info = build_database(queries, args.db_seqs, seed=rank)
     res_cells = segment_cells(db)
+    from sseqs_b200 import tune
+    tuned = tune.autotune([len(q) for q in queries], db.batches[0])
     warm, timed = step_queries(queries, args.steps, args.warmup)
     for q in warm:
         run_step(M, q, db, world=world, rank=rank)
@@ -282,9 +286,13 @@ def bench_b200(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    peak = dpx_peak()
-    ops_per_cell = 3.5                                   # 7 DPX lane-ops per 2 cells (affine)
-    achieved = aff_cells * ops_per_cell / (sum(aff_ms) * 1e-3)
+    alu_peak = measured_peak("sseqs_dpx_peak")
+    dual_peak = measured_peak("sseqs_int16x2_peak")
+    aff_rate = aff_cells / (sum(aff_ms) * 1e-3)          # cells/s of the affine launches
+    # The affine kernel issues 3.5 ALU-pipe (max-type DPX) + 2 FMA-pipe
+    # (int16x2 add) instructions per int16x2 word, i.e. per 2 cells; the ALU
+    # pipe is its limit.
+    achieved = aff_rate * 3.5 / 2
     out = {
         "metric": "SW GCUPS on 1 B200",
         "value": round(gcups, 1),
@@ -311,16 +319,25 @@ def bench_b200(args):
         "queries_per_s": round(len(timed) * world / (ms * 1e-3), 3),
         "gcups_affine_kernel": round(aff_cells / (sum(aff_ms) * 1e-3) / 1e9, 1),
         "roofline": {
-            "bound": "dpx",
+            "bound": "int-pipe (ALU, DPX)",
             "kernel": "sw_stream_kernel<affine> (dominant launch of the step)",
             "achieved": round(achieved / 1e9, 1),
-            "peak": round(peak / 1e9, 1),
+            "peak": round(alu_peak / 1e9, 1),
             "unit": "Gop/s",
-            "frac": round(achieved / peak, 4),
+            "frac": round(achieved / alu_peak, 4),
             "traffic": None,
-            "ops_model": "7 int16x2 DPX lane-ops per 2 cells (affine)",
-            "peak_source": "sseqs_dpx_peak, measured in this run (int16x2 DPX issue rate)",
+            "ops_model": "3.5 ALU-pipe DPX int16x2 instructions per 2 cells (affine kernel)",
+            "peak_source": "sseqs_dpx_peak measured in this run: ALU-pipe int16x2 DPX issue rate",
+            "dual_pipe": {"achieved": round(aff_rate * 5.5 / 2 / 1e9, 1),
+                          "peak": round(dual_peak / 1e9, 1),
+                          "frac": round(aff_rate * 5.5 / 2 / dual_peak, 4),
+                          "ops_model": "5.5 int16x2 instructions per 2 cells (3.5 ALU + 2 FMA)"},
+            "survey_model": {"peak_cells_per_s": round(alu_peak * 2 / 7 / 1e9, 1),
+                             "frac": round(aff_rate / (alu_peak * 2 / 7), 4),
+                             "ops_model": "7 DPX ops per 2 cells"},
         },
+        "autotune": {f"{'affine' if a else 'linear'}_tpt{t}": ("wide" if w else "narrow")
+                     for (a, t), w in sorted(tuned.items())},
         "e2e": {"value": round(e2e_gcups, 1), "unit": "GCUPS",
                 "h2d_bytes_per_step": int(h2d / len(timed)),
                 "d2h_bytes_per_step": int(d2h / len(timed)),

@@ -178,9 +178,23 @@ int sseqs_prefilter(const uint8_t* ascii, const int64_t* offsets, const int32_t*
  * word the kernel may write so that its work is not optimised away.
  * Synchronises on `stream`.  No reference counterpart (measurement aid). */
 int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream);
+/* int16x2 issue rate over both int pipes: max-type DPX instructions (ALU
+ * pipe) interleaved with int16x2 adds (FMA pipe), in lane-instructions per
+ * second.  Synchronises.  No reference counterpart (measurement aid). */
+int sseqs_int16x2_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream);
 /* Number of kernels this library has enqueued since it was loaded (every
  * launch site counts itself).  No reference counterpart. */
 int64_t sseqs_launch_count(void);
+
+/* ----------------------------------------------------------- tuning */
+/* The score kernel has two lane layouts for stripe widths tpt =
+ * ceil(query_len/32) <= 16: narrow (wide = 0, default) and wide (wide = 1:
+ * twice the columns per lane, twice the targets per warp).  Selects the one
+ * used for (affine, tpt); both give identical scores.  No reference
+ * counterpart (the autotuner of the batched path sets it). */
+int sseqs_sw_set_variant(int affine, int tpt, int wide);
+/* int16x2 words per lane of a variant (for reports); -1 if out of range. */
+int sseqs_sw_variant_words(int affine, int tpt, int wide);
 
 #ifdef __cplusplus
 }

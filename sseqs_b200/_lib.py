@@ -45,6 +45,9 @@ _SIGNATURES = {
     "sseqs_prefilter": (_I, [_P, _P, _P, _I64, _P, _I, _P, _P, _I, _I, _P, _P, _SZ, _P]),
     "sseqs_dpx_peak": (_I, [_P, ctypes.POINTER(_D), _P]),
     "sseqs_launch_count": (_I64, []),
+    "sseqs_int16x2_peak": (_I, [_P, ctypes.POINTER(_D), _P]),
+    "sseqs_sw_set_variant": (_I, [_I, _I, _I]),
+    "sseqs_sw_variant_words": (_I, [_I, _I, _I]),
 }
 
 _lock = threading.Lock()

@@ -1,47 +1,9 @@
-// Score-only Smith-Waterman (linear and affine gaps) for sm_100a.
-//
-// Semantics are those of the reference kernels sseqs/sw.cu:55-179 (linear)
-// and sseqs/sw.cu:182-325 (affine): the query is cut into 32 stripes of
-// TPT = ceil(Lq/32) columns; inside a row the horizontal dependency restarts
-// at the first column of every stripe (H(i, j-1) := 0 there), while the
-// diagonal dependency crosses stripes.  Because the rows of all stripes are
-// independent of each other inside one row, the stripes can be evaluated in
-// any lane mapping.
-//
-// B200 mapping.  Two stripes of the same target share one 32-bit register as
-// int16x2 (lo = stripe 2m, hi = stripe 2m+1).  A lane holds W such words per
-// column, so a target occupies G = 32/(2W) lanes and a warp scores 2W
-// targets side by side.  The query profile (score of each residue class
-// against every column, already packed as the lane's int16x2 words) sits in
-// shared memory; a lane fetches its row of it with 128-bit loads.
-//
-// Every int16x2 instruction used here issues at half rate on its pipe: the
-// max-type DPX instructions (__vimax3_s16x2_relu, __viaddmax_s16x2_relu) on
-// the ALU pipe, the int16x2 add/sub (__vadd2, __vsub2) on the FMA pipe.  A
-// scheduler issues one instruction per clock, so the recurrences are written
-// to spread work over both pipes:
-//   affine, per word-column (2 cells): M' = D_diag + s, Mo = M' - open (FMA);
-//     Ix = max(Ix_left - ext, Mo_left, 0), D = max(M', Ix, Iy, 0),
-//     next-row Iy = max(Iy - ext, Mo, 0), half a running max (ALU)
-//     -> 3.5 ALU + 2 FMA;
-//   linear, with the state carried as H + gap: u = Hg_diag + (s - gap) (FMA),
-//     H = max(u, Hg_up, Hg_left, 0), half a running max (ALU),
-//     Hg = H + gap (FMA)  -> 1.5 ALU + 2 FMA.
-// M' is left unclamped: it only enters maxima that also hold 0.  All cell
-// values are >= 0 and at most 11 * Lq <= 22528, so int16 lanes cannot
-// overflow for Lq <= 2048 (no int32 re-run is ever needed); the profile's
-// padding words (-32768 + open, or -16384) keep every intermediate inside
-// int16 and can never raise a score.
-//
-// Targets are streamed: each lane group walks a contiguous range of targets
-// four rows at a time, the four bytes of the next quad prefetched with two
-// aligned 32-bit loads; when a target ends (rows past its end are padding
-// rows) the group writes its score, resets its state and moves on while the
-// other groups of the warp keep going.
-#include <algorithm>
+// Score-only Smith-Waterman: dispatch, the exact fallback kernel and the C
+// ABI.  The fast int16x2 kernel is the template in sw_kernel.cuh (see there
+// for its design), instantiated per stripe width in sw_inst_*.cu.
 #include <mutex>
 
-#include "common.cuh"
+#include "sw_kernel.cuh"
 
 namespace sseqs {
 
@@ -57,274 +19,7 @@ int device_sm_count() {
   return cached[dev];
 }
 
-namespace {
-
-constexpr int kMaxQuery = 2048;
-constexpr int kThreads = 128;
-
-struct SwArgs {
-  const uint8_t* q;       // query residue classes
-  int Lq;
-  const int32_t* idx;     // target -> window index g (nullable: g = g0 + t)
-  int32_t g0;
-  int64_t n;              // number of targets
-  const uint8_t* ascii;   // target bytes
-  const int32_t* starts;  // window table (reference semantics)
-  int skip;               // bytes not scored at the start of every window
-  int32_t* out;
-  int p0, p1;             // linear: gap; affine: open, extend
-};
-
-// Window of one target (sseqs/sw.cu:66-77): rows [pos, end), or no rows and
-// an immediate result (-1 for an empty or inverted window, 0 otherwise).
-struct Win {
-  int64_t pos, end;
-  int32_t res;
-  bool rows;
-};
-
-__device__ __forceinline__ Win window_of(const SwArgs& a, int64_t t) {
-  const int32_t g = a.idx ? a.idx[t] : (int32_t)(a.g0 + t);
-  const int64_t base = (g == 0) ? -1 : (int64_t)a.starts[g - 1];
-  const int64_t len = (int64_t)a.starts[g] - base - 1;
-  Win w;
-  w.pos = base + 1 + a.skip;
-  w.end = base + 1 + len;
-  if (len == 0 || len < -1) {
-    w.rows = false;
-    w.res = -1;
-  } else {
-    w.rows = w.pos < w.end;
-    w.res = 0;
-  }
-  return w;
-}
-
-__device__ __forceinline__ int score_of(const uint8_t* q, int Lq, int cls, int j) {
-  if (j >= Lq || cls == kClsPad) return kNeg;
-  if (cls >= kNumAA) return -4;
-  const int qc = q[j];
-  return qc < kNumAA ? blosum62(cls, qc) : -4;
-}
-
-template <int TPT>
-constexpr int words_for() {
-  return TPT == 1 ? 16 : TPT == 2 ? 8 : TPT <= 4 ? 4 : TPT <= 8 ? 2 : 1;
-}
-
-template <int TPT, int W>
-struct Layout {
-  static constexpr int G = 32 / (2 * W);    // lanes per target
-  static constexpr int GPW = 2 * W;         // targets per warp
-  static constexpr int NWD = W * TPT;       // profile words per lane and row
-  static constexpr int NV = (NWD + 3) / 4;  // 128-bit loads per lane and row
-  static constexpr int LWP = ((NV % 2) ? NV : NV + 1) * 4;  // odd # of uint4
-  static constexpr int CLS = G * LWP;       // words per residue class
-  static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
-};
-
-template <int TPT, int W, bool AFF>
-__global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
-  using L = Layout<TPT, W>;
-  constexpr int G = L::G;
-  extern __shared__ uint4 smem4[];
-  uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);
-  uint8_t* lut = reinterpret_cast<uint8_t*>(prof + kNumCls * L::CLS);
-
-  // Profile words.  Affine: s (real columns), -32768 + open (padding), so
-  // that M' - open never leaves int16.  Linear: s - gap (the state carries
-  // H + gap), -16384 for padding.  Padding never raises a score.
-  const int pad = AFF ? kNeg + a.p0 : -16384;
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = ascii_class((uint8_t)i);
-  for (int i = threadIdx.x; i < kNumCls * L::CLS; i += blockDim.x) {
-    const int c = i / L::CLS, r = i - c * L::CLS;
-    const int gl = r / L::LWP, v = r - gl * L::LWP;
-    uint32_t word = pack2(pad, pad);
-    if (v < L::NWD) {
-      const int w = v / TPT, k = v - w * TPT;
-      const int j = (gl * 2 * W + 2 * w) * TPT + k;
-      int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + TPT);
-      s0 = (s0 == kNeg) ? pad : (AFF ? s0 : s0 - a.p0);
-      s1 = (s1 == kNeg) ? pad : (AFF ? s1 : s1 - a.p0);
-      word = pack2(s0, s1);
-    }
-    prof[i] = word;
-  }
-  __syncthreads();
-
-  const int lane = threadIdx.x & 31;
-  const int grp = lane / G;
-  const int gl = lane - grp * G;
-  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t ngroups = nwarps * L::GPW;
-  const int64_t gid = wid * L::GPW + grp;
-  int64_t t = (a.n * gid) / ngroups;
-  const int64_t t_hi = (a.n * (gid + 1)) / ngroups;
-
-  const uint32_t gap2 = pack2(a.p0, a.p0);    // linear gap, -16384 <= gap <= 0
-  const uint32_t open2 = pack2(a.p0, a.p0);   // affine open, 0 <= open <= 16384
-  const uint32_t next2 = pack2(-a.p1, -a.p1); // affine -extend, 0 <= extend <= 16384
-  // state at row -1: H = 0 (linear state is H + gap), D = Iy = 0 (affine)
-  const uint32_t init = AFF ? 0u : gap2;
-
-  uint32_t S[W][TPT];                 // linear: H(i-1,.) + gap   affine: D(i-1,.)
-  uint32_t Y[AFF ? W : 1][TPT];       // affine: Iy(i,.) carried into row i
-  uint32_t best = 0;
-  auto reset = [&]() {
-    best = 0;
-#pragma unroll
-    for (int w = 0; w < W; ++w)
-#pragma unroll
-      for (int k = 0; k < TPT; ++k) {
-        S[w][k] = init;
-        if constexpr (AFF) Y[w][k] = 0;
-      }
-  };
-  reset();
-
-  // one DP row for every group of the warp (warp-uniform)
-  auto row = [&](int cls) {
-    const uint4* pr = reinterpret_cast<const uint4*>(prof + cls * L::CLS + gl * L::LWP);
-    uint32_t s[L::NV * 4];
-#pragma unroll
-    for (int v = 0; v < L::NV; ++v) {
-      const uint4 x = pr[v];
-      s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
-    }
-    uint32_t from_left = __shfl_up_sync(0xffffffffu, S[W - 1][TPT - 1], 1, G);
-    if (gl == 0) from_left = init;                  // column -1 of stripe 0
-    uint32_t din[W];
-#pragma unroll
-    for (int w = 0; w < W; ++w)
-      din[w] = __byte_perm(w == 0 ? from_left : S[w - 1][TPT - 1], S[w][TPT - 1], 0x5432);
-    uint32_t pend = 0;
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-      uint32_t diag = din[w];
-      if constexpr (!AFF) {
-        // state Hg = H + gap:  H = max(Hg_diag + (s - gap), Hg_up, Hg_left, 0)
-        // (Hg_left = gap at the first column of a stripe)
-        uint32_t hg_left = 0;
-#pragma unroll
-        for (int k = 0; k < TPT; ++k) {
-          const uint32_t up = S[w][k];
-          const uint32_t u = __vadd2(diag, s[w * TPT + k]);                 // FMA pipe
-          const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
-                                      : __vimax3_s16x2_relu(u, up, hg_left); // ALU pipe
-          hg_left = __vadd2(h, gap2);                                       // FMA pipe
-          diag = up;
-          S[w][k] = hg_left;
-          if (((w * TPT + k) & 1) == 0) pend = h;
-          else best = __vimax3_s16x2(best, pend, h);
-        }
-      } else {
-        // M' = D_diag + s (unclamped), Mo = M' - open          FMA pipe
-        // Ix = max(Ix_left - ext, Mo_left, 0)   (0 at k = 0)  ALU
-        // D  = max(M', Ix, Iy, 0)                             ALU
-        // Iy(next row) = max(Iy - ext, Mo, 0)                 ALU
-        uint32_t X = 0, mo_left = 0;
-#pragma unroll
-        for (int k = 0; k < TPT; ++k) {
-          const uint32_t mp = __vadd2(diag, s[w * TPT + k]);
-          const uint32_t mo = __vsub2(mp, open2);
-          if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
-          const uint32_t y = Y[w][k];
-          const uint32_t D = (k > 0) ? __vimax3_s16x2_relu(mp, X, y) : __vimax_s16x2_relu(mp, y);
-          Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
-          diag = S[w][k];
-          S[w][k] = D;
-          mo_left = mo;
-          if (((w * TPT + k) & 1) == 0) pend = D;
-          else best = __vimax3_s16x2(best, pend, D);
-        }
-      }
-    }
-    if ((L::NWD & 1) != 0) best = __vimax_s16x2_relu(best, pend);
-  };
-
-  // ---- target bytes: four rows at a time from two aligned 32-bit words.
-  // A word is loaded only when it holds a byte of the window being read, so
-  // no load leaves the windows' own 4-byte words.
-  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
-  const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
-  const int64_t aoff = (int64_t)(au & 3);
-  struct Quad { uint32_t w0, w1; };
-  auto fetch = [&](int64_t p, int64_t e) -> Quad {
-    const int64_t ap = p + aoff;
-    const int64_t wi = ap >> 2;
-    Quad q;
-    q.w0 = __ldg(abase + wi);
-    q.w1 = ((wi + 1) << 2) < e + aoff ? __ldg(abase + wi + 1) : 0u;
-    return q;
-  };
-  uint32_t c0 = kClsPad, c1 = kClsPad, c2 = kClsPad, c3 = kClsPad;
-  auto classes = [&](const Quad& q, int64_t p, int64_t e) {
-    const uint32_t raw = __funnelshift_r(q.w0, q.w1, (uint32_t)((p + aoff) & 3) * 8u);
-    c0 = p + 0 < e ? lut[raw & 0xffu] : kClsPad;
-    c1 = p + 1 < e ? lut[(raw >> 8) & 0xffu] : kClsPad;
-    c2 = p + 2 < e ? lut[(raw >> 16) & 0xffu] : kClsPad;
-    c3 = p + 3 < e ? lut[raw >> 24] : kClsPad;
-  };
-
-  // ---- target bookkeeping (group-uniform) ----
-  Win cur, nxt;
-  bool active = false, nxt_ok = false;
-  auto start_from = [&](int64_t tt) {   // first target at or after tt with rows
-    active = false;
-    nxt_ok = false;
-    t = tt;
-    while (t < t_hi) {
-      cur = window_of(a, t);
-      if (cur.rows) { active = true; break; }
-      if (gl == 0) a.out[t] = cur.res;
-      ++t;
-    }
-    if (active && t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
-  };
-  start_from(t);
-  if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
-
-  while (__any_sync(0xffffffffu, active)) {
-    // prefetch the bytes of the next quad of this group
-    Quad pf{0u, 0u};
-    bool pf_nxt = false;
-    if (active) {
-      if (cur.pos + 4 < cur.end) pf = fetch(cur.pos + 4, cur.end);
-      else if (nxt_ok && nxt.rows) { pf = fetch(nxt.pos, nxt.end); pf_nxt = true; }
-    }
-    row(c0);
-    row(c1);
-    row(c2);
-    row(c3);
-    if (active) {
-      cur.pos += 4;
-      if (cur.pos >= cur.end) {
-        // target finished (rows past its end were padding rows)
-        int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
-#pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
-        if (gl == 0) a.out[t] = v;
-        reset();
-        if (pf_nxt) {
-          ++t;
-          cur = nxt;
-          nxt_ok = false;
-          if (t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
-          classes(pf, cur.pos, cur.end);
-        } else {
-          start_from(t + 1);
-          if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
-          else c0 = c1 = c2 = c3 = kClsPad;
-        }
-      } else {
-        classes(pf, cur.pos, cur.end);
-      }
-    }
-  }
-}
-
+namespace sw {
 // Exact restatement for gap parameters outside the fast kernel's domain
 // (linear gap > 0, affine open/extend < 0): one thread per target, cells
 // stored as uint16 (linear) / int16 (affine) exactly as sseqs/sw.cu does.
@@ -380,69 +75,52 @@ __global__ void fill_kernel(int32_t* out, int64_t n, int32_t v) {
 }
 
 // ---------------------------------------------------------------- dispatch
-using KernelFn = void (*)(SwArgs);
-
-struct KernelInfo {
-  KernelFn fn = nullptr;
-  size_t smem = 0;
-  int groups_per_block = 0;
-};
-
-template <int TPT, bool AFF>
-KernelInfo make_info() {
-  constexpr int W = words_for<TPT>();
-  KernelInfo k;
-  k.fn = sw_stream_kernel<TPT, W, AFF>;
-  k.smem = Layout<TPT, W>::smem;
-  k.groups_per_block = (kThreads / 32) * Layout<TPT, W>::GPW;
-  return k;
-}
-
-template <bool AFF, int... T>
-void fill_table(KernelInfo* tab, std::integer_sequence<int, T...>) {
-  ((tab[T] = make_info<T + 1, AFF>()), ...);
+const Tables& tables() {
+  static Tables t;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    register_1_16(t);
+    register_17_32(t);
+    register_33_48(t);
+    register_49_64(t);
+  });
+  return t;
 }
 
 struct Cache {
   std::mutex mu;
-  int max_blocks[2][64][64] = {};  // [affine][TPT-1][device]
+  int max_blocks[2][2][64][64] = {};  // [variant][affine][TPT-1][device]
+  int variant[2][64] = {};            // chosen variant per [affine][TPT-1]
 };
 Cache& cache() {
   static Cache c;
   return c;
 }
 
-const KernelInfo& info_for(int tpt, bool aff) {
-  static KernelInfo lin[64], afn[64];
-  static std::once_flag once;
-  std::call_once(once, [] {
-    fill_table<false>(lin, std::make_integer_sequence<int, 64>{});
-    fill_table<true>(afn, std::make_integer_sequence<int, 64>{});
-  });
-  return aff ? afn[tpt - 1] : lin[tpt - 1];
-}
-
 int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
   const int tpt = (a.Lq + 31) / 32;
-  const KernelInfo& k = info_for(tpt, aff);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
-  int blocks_per_sm;
+  int blocks_per_sm, var;
+  const KernelInfo* kp;
   {
     std::lock_guard<std::mutex> lk(cache().mu);
-    int& mb = cache().max_blocks[aff][tpt - 1][dev];
+    var = cache().variant[aff][tpt - 1];
+    kp = &tables().k[var][aff][tpt - 1];
+    int& mb = cache().max_blocks[var][aff][tpt - 1][dev];
     if (mb == 0) {
-      if (cudaFuncSetAttribute((const void*)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)k.smem) != cudaSuccess)
+      if (cudaFuncSetAttribute((const void*)kp->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kp->smem) != cudaSuccess)
         return SSEQS_ERR_CUDA;
       int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)k.fn, kThreads,
-                                                        k.smem) != cudaSuccess || nb < 1)
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kp->fn, kThreads,
+                                                        kp->smem) != cudaSuccess || nb < 1)
         return SSEQS_ERR_CUDA;
       mb = nb;
     }
     blocks_per_sm = mb;
   }
+  const KernelInfo& k = *kp;
   const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
   const int64_t need = (a.n + k.groups_per_block - 1) / k.groups_per_block;
   const int grid = (int)std::max<int64_t>(1, std::min(full, need));
@@ -494,10 +172,54 @@ __global__ void dpx_peak_kernel(uint32_t* sink, int iters, uint32_t seed) {
   if (acc == 0x9e3779b9u) sink[0] = acc;   // practically never taken
 }
 
-}  // namespace
+// int16x2 issue peak over both pipes: independent max-type DPX chains (ALU
+// pipe) interleaved with int16x2 add chains (FMA pipe).
+__global__ void int16x2_peak_kernel(uint32_t* sink, int iters, uint32_t seed) {
+  uint32_t x[8], y[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    x[i] = seed * (threadIdx.x + 7 * i + 1);
+    y[i] = seed ^ (blockIdx.x + 13 * i);
+  }
+  const uint32_t d = seed | 0x00010001u, e = seed >> 3;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      x[i] = __vimax3_s16x2_relu(x[i], d, e ^ (uint32_t)i);
+      y[i] = __vadd2(y[i], d);
+    }
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc ^= x[i] ^ y[i];
+  if (acc == 0x9e3779b9u) sink[0] = acc;   // practically never taken
+}
+
+int time_peak(void (*kern)(uint32_t*, int, uint32_t), uint32_t* sink, double* out,
+              cudaStream_t stream) {
+  const int blocks = device_sm_count() * 8, threads = 256, iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return SSEQS_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return SSEQS_ERR_CUDA; }
+  { kern<<<blocks, threads, 0, stream>>>(sink, iters / 8, 0x12345u); count_launches(1); }
+  cudaEventRecord(e0, stream);
+  { kern<<<blocks, threads, 0, stream>>>(sink, iters, 0x12345u); count_launches(1); }
+  cudaEventRecord(e1, stream);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess || ms <= 0.f) return SSEQS_ERR_CUDA;
+  *out = (double)blocks * threads * iters * 16.0 / (ms * 1e-3);
+  return SSEQS_OK;
+}
+
+}  // namespace sw
 }  // namespace sseqs
 
 using namespace sseqs;
+using namespace sseqs::sw;
 
 extern "C" int sseqs_max_query_len(void) { return kMaxQuery; }
 
@@ -528,20 +250,22 @@ extern "C" int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len
 
 extern "C" int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream) {
   if (!lane_ops_per_s || !sink) return SSEQS_ERR_ARG;
-  const int blocks = device_sm_count() * 8, threads = 256, iters = 1 << 14;
-  cudaEvent_t e0, e1;
-  if (cudaEventCreate(&e0) != cudaSuccess) return SSEQS_ERR_CUDA;
-  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return SSEQS_ERR_CUDA; }
-  { dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters / 8, 0x12345u); count_launches(1); }   // warm-up
-  cudaEventRecord(e0, stream);
-  { dpx_peak_kernel<<<blocks, threads, 0, stream>>>(sink, iters, 0x12345u); count_launches(1); }
-  cudaEventRecord(e1, stream);
-  cudaError_t err = cudaEventSynchronize(e1);
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (err != cudaSuccess || ms <= 0.f) return SSEQS_ERR_CUDA;
-  *lane_ops_per_s = (double)blocks * threads * iters * 16.0 / (ms * 1e-3);
+  return time_peak(dpx_peak_kernel, sink, lane_ops_per_s, stream);
+}
+
+extern "C" int sseqs_int16x2_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream) {
+  if (!lane_ops_per_s || !sink) return SSEQS_ERR_ARG;
+  return time_peak(int16x2_peak_kernel, sink, lane_ops_per_s, stream);
+}
+
+extern "C" int sseqs_sw_set_variant(int affine, int tpt, int wide) {
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1)) return SSEQS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(cache().mu);
+  cache().variant[affine ? 1 : 0][tpt - 1] = wide;
   return SSEQS_OK;
+}
+
+extern "C" int sseqs_sw_variant_words(int affine, int tpt, int wide) {
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1)) return -1;
+  return tables().k[wide][affine ? 1 : 0][tpt - 1].words;
 }

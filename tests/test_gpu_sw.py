@@ -137,3 +137,27 @@ def test_sw_api_matches_oracle():
     exp = O.sw_affine(O.encode_query(query), np.arange(len(targets), dtype=np.int32),
                       ascii, starts, 11, 1)
     np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("Lq", [17, 40, 100, 200, 300, 500])
+def test_wide_layout_matches_oracle(Lq):
+    """Both lane layouts of a stripe width give the oracle's scores."""
+    S = importlib.import_module("sseqs_b200.sw")
+    from sseqs_b200 import tune
+    query, q, ascii, starts = _case(5000 + Lq, Lq, 400, extra="XB@")
+    good = np.arange(len(starts), dtype=np.int32)
+    qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
+    tpt = tune.tpt_of(Lq)
+    try:
+        for wide in (0, 1):
+            tune.set_variant(False, tpt, wide)
+            tune.set_variant(True, tpt, wide)
+            np.testing.assert_array_equal(
+                S.sw_cuda_blosum62(qd, gd, ad, sd, gap_penalty_param=-1).cpu().numpy(),
+                O.sw_linear(q, good, ascii, starts, -1, NT))
+            np.testing.assert_array_equal(
+                S.sw_cuda_affine(qd, gd, ad, sd, 11, 1).cpu().numpy(),
+                O.sw_affine(q, good, ascii, starts, 11, 1, NT))
+    finally:
+        tune.set_variant(False, tpt, 0)
+        tune.set_variant(True, tpt, 0)
