@@ -282,6 +282,7 @@ def bench_b200(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     cells = 0
+    exact_rows = {}
     for q in timed:
         rows, _ = run_step(M, q, db, timer=timer, world=world, rank=rank)
         exact_rows.setdefault(q, rows)
@@ -296,7 +297,6 @@ def bench_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     total_cells = cells * world
-    exact_rows = {}
     gcups = total_cells / (ms * 1e-3) / 1e9
     aff_ms = [a.elapsed_time(b) for a, b in aff_events]
     aff_cells = sum(len(q) * res_cells for q in timed)
