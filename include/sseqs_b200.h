@@ -30,7 +30,9 @@ enum {
   SSEQS_ERR_ARG = 1,          /* invalid argument (null pointer, bad size)   */
   SSEQS_ERR_UNSUPPORTED = 2,  /* valid input outside the supported range     */
   SSEQS_ERR_CUDA = 3,         /* a CUDA runtime call or launch failed        */
-  SSEQS_ERR_WORKSPACE = 4     /* workspace missing or too small              */
+  SSEQS_ERR_WORKSPACE = 4,    /* workspace missing or too small              */
+  SSEQS_ERR_CAPACITY = 5      /* input larger than a fixed-capacity entry
+                                 point can hold (sseqs_topk_static)          */
 };
 
 /* Human-readable text for a status code (host, static storage). */
@@ -127,6 +129,24 @@ int sseqs_segment_table(const uint8_t* ascii, int64_t n, const int32_t* delim,
 size_t sseqs_topk_workspace_bytes(int64_t n);
 int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, int32_t* out_idx,
                void* workspace, size_t ws_bytes, cudaStream_t stream);
+
+/* Same selection as sseqs_topk, for callers that must not allocate device
+ * memory: code whose GPU memory is owned by another allocator (a framework's
+ * caching pool, a server's fixed budget) and may not take memory behind its
+ * back, or a latency-critical caller that cannot afford the stalls that
+ * cudaMalloc / cudaFree can cause.  The caller passes keys and out_idx only;
+ * the scratch is a fixed array inside this library (about 66 KB per GPU that
+ * loads the library, held until the process exits), so n is limited to
+ * SSEQS_TOPK_STATIC_MAX_N keys -- larger n returns SSEQS_ERR_CAPACITY.  The
+ * first call on a device looks up that array's device address (with the
+ * device current); make that first call before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Nothing
+ * is allocated, neither here nor in the kernels.
+ * This entry point has no counterpart in the reference. */
+#define SSEQS_TOPK_STATIC_MAX_N (1 << 24)
+int sseqs_topk_static(const void* keys, int key_type, int64_t n, int64_t k, int32_t* out_idx,
+                      cudaStream_t stream);
 
 /* Hit strings of selected segments: row r of out (width bytes) receives
  * ascii[offsets[g] .. offsets[g] + min(width, lengths[g])), g = idx[r], the

@@ -17,6 +17,8 @@ extern "C" const char* sseqs_status_string(int status) {
     case SSEQS_ERR_UNSUPPORTED: return "input outside the supported range";
     case SSEQS_ERR_CUDA: return "CUDA runtime error";
     case SSEQS_ERR_WORKSPACE: return "workspace missing or too small";
+    case SSEQS_ERR_CAPACITY:
+      return "input larger than the fixed scratch capacity of this entry point";
     default: return "unknown status";
   }
 }

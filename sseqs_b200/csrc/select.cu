@@ -15,6 +15,7 @@
 // 8-bit radix passes (shared-memory histograms merged with 256 global atomics
 // per block) before compacting.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -487,5 +488,80 @@ extern "C" int sseqs_gather_windows(const uint8_t* ascii, const int64_t* offsets
   const int grid = (int)std::min<int64_t>(n, (int64_t)device_sm_count() * 16);
   { gather_windows_kernel<<<grid, 128, 0, stream>>>(ascii, offsets, lengths, idx, n, width, out,
                                                   out_len); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+// ------------------------------------------------ top-k without allocation
+// Scratch of sseqs_topk_static: the same control block and per-tile counters
+// as sseqs_topk's workspace, in a fixed array that every GPU loading this
+// library holds until the process exits (about 66 KB).  Host code may not
+// pass this symbol to a kernel (on the host it names a stand-in, not device
+// memory); it uses the device address fetched below.
+namespace {
+constexpr int64_t kStaticTopkMaxN = SSEQS_TOPK_STATIC_MAX_N;
+constexpr int64_t kStaticTopkTiles = kStaticTopkMaxN / kTile;
+constexpr size_t kStaticCtlBytes = (sizeof(TopkCtl) + 255) & ~(size_t)255;
+constexpr size_t kStaticScratchBytes =
+    kStaticCtlBytes + 2 * sizeof(int64_t) * (size_t)kStaticTopkTiles;
+static_assert(kStaticTopkMaxN % kTile == 0, "capacity must be whole tiles");
+
+static __device__ __align__(256) unsigned char g_topk_scratch[kStaticScratchBytes];
+
+// Device address of g_topk_scratch for the current device, looked up once
+// per device (with that device current) and cached.
+int static_topk_scratch(unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* addr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SSEQS_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_topk_scratch) != cudaSuccess || !p) return SSEQS_ERR_CUDA;
+    addr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = addr[dev];
+  return SSEQS_OK;
+}
+}  // namespace
+
+extern "C" int sseqs_topk_static(const void* keys, int key_type, int64_t n, int64_t k,
+                                 int32_t* out_idx, cudaStream_t stream) {
+  if (n < 0 || k < 0 || k > n || (key_type != 0 && key_type != 1)) return SSEQS_ERR_ARG;
+  if (n > kStaticTopkMaxN) return SSEQS_ERR_CAPACITY;
+  if (k == 0) return SSEQS_OK;
+  if (!keys || !out_idx) return SSEQS_ERR_ARG;
+  if (k == n) {
+    { iota_kernel<<<grid_for(n), kSelThreads, 0, stream>>>(out_idx, n); count_launches(1); }
+    return status_of(cudaGetLastError());
+  }
+  unsigned char* base = nullptr;
+  const int st = static_topk_scratch(&base);
+  if (st != SSEQS_OK) return st;
+  // The control block is rewritten by topk_init_kernel at the start of every
+  // call, and every counter slot a call reads is written earlier in the same
+  // call, so nothing left over from a previous call is read.
+  TopkCtl* ctl = reinterpret_cast<TopkCtl*>(base);
+  int64_t* cg = reinterpret_cast<int64_t*>(base + kStaticCtlBytes);
+  int64_t* ce = cg + kStaticTopkTiles;
+  const int64_t tiles = (n + kTile - 1) / kTile;
+  const int grid = grid_for(n);
+  const int hgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + kSelThreads - 1) / kSelThreads,
+                                                                (int64_t)device_sm_count() * 4));
+  { topk_init_kernel<<<1, 256, 0, stream>>>(ctl, k); count_launches(1); }
+  const int first_shift = key_type == 0 ? 24 : 8;
+  for (int shift = first_shift; shift >= 0; shift -= 8) {
+    if (key_type == 0)
+      { topk_hist_kernel<0><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift); count_launches(1); }
+    else
+      { topk_hist_kernel<1><<<hgrid, kSelThreads, 0, stream>>>(keys, n, ctl, shift); count_launches(1); }
+    { topk_pick_kernel<<<1, 256, 0, stream>>>(ctl, shift); count_launches(1); }
+  }
+  if (key_type == 0) { topk_count_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce); count_launches(1); }
+  else { topk_count_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(cg, tiles, nullptr); count_launches(1); }
+  { scan_counts_kernel<<<1, kSelThreads, 0, stream>>>(ce, tiles, nullptr); count_launches(1); }
+  if (key_type == 0) { topk_scatter_kernel<0><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx); count_launches(1); }
+  else { topk_scatter_kernel<1><<<grid, kSelThreads, 0, stream>>>(keys, n, ctl, cg, ce, out_idx); count_launches(1); }
   return status_of(cudaGetLastError());
 }
