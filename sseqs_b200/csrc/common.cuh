@@ -19,30 +19,38 @@ constexpr int16_t kNeg = -32768;
 
 // BLOSUM62 in the order above (published matrix; the same values as
 // sseqs/sw.cu:7-29).  Row = target residue, column = query residue; the
-// matrix is symmetric.
+// matrix is symmetric.  Device code reads the constant-memory copy (a
+// function-local table would be rebuilt on the stack at every call).
+#define SSEQS_BLOSUM62_VALUES \
+  4, -1, -2, -2, 0,  -1, -1, 0,  -2, -1, -1, -1, -1, -2, -1, 1,  0,  -3, -2, 0, \
+  -1, 5, 0,  -2, -3, 1,  0,  -2, 0,  -3, -2, 2,  -1, -3, -2, -1, -1, -3, -2, -3, \
+  -2, 0, 6,  1,  -3, 0,  0,  0,  1,  -3, -3, 0,  -2, -3, -2, 1,  0,  -4, -2, -3, \
+  -2, -2, 1, 6,  -3, 0,  2,  -1, -1, -3, -4, -1, -3, -3, -1, 0,  -1, -4, -3, -3, \
+  0, -3, -3, -3, 9,  -3, -4, -3, -3, -1, -1, -3, -1, -2, -3, -1, -1, -2, -2, -1, \
+  -1, 1, 0,  0,  -3, 5,  2,  -2, 0,  -3, -2, 1,  0,  -3, -1, 0,  -1, -2, -1, -2, \
+  -1, 0, 0,  2,  -4, 2,  5,  -2, 0,  -3, -3, 1,  -2, -3, -1, 0,  -1, -3, -2, -2, \
+  0, -2, 0,  -1, -3, -2, -2, 6,  -2, -4, -4, -2, -3, -3, -2, 0,  -2, -2, -3, -3, \
+  -2, 0, 1,  -1, -3, 0,  0,  -2, 8,  -3, -3, -1, -2, -1, -2, -1, -2, -2, 2,  -3, \
+  -1, -3, -3, -3, -1, -3, -3, -4, -3, 4, 2,  -3, 1,  0,  -3, -2, -1, -3, -1, 3, \
+  -1, -2, -3, -4, -1, -2, -3, -4, -3, 2, 4,  -2, 2,  0,  -3, -2, -1, -2, -1, 1, \
+  -1, 2, 0,  -1, -3, 1,  1,  -2, -1, -3, -2, 5,  -1, -3, -1, 0,  -1, -3, -2, -2, \
+  -1, -1, -2, -3, -1, 0, -2, -3, -2, 1,  2,  -1, 5,  0,  -2, -1, -1, -1, -1, 1, \
+  -2, -3, -3, -3, -2, -3, -3, -3, -1, 0, 0,  -3, 0,  6,  -4, -2, -2, 1,  3,  -1, \
+  -1, -2, -2, -1, -3, -1, -1, -2, -2, -3, -3, -1, -2, -4, 7, -1, -1, -4, -3, -2, \
+  1, -1, 1,  0,  -1, 0,  0,  0,  -1, -2, -2, 0,  -1, -2, -1, 4,  1,  -3, -2, -2, \
+  0, -1, 0,  -1, -1, -1, -1, -2, -2, -1, -1, -1, -1, -2, -1, 1,  5,  -2, -2, 0, \
+  -3, -3, -4, -4, -2, -2, -3, -2, -2, -3, -2, -3, -1, 1, -4, -3, -2, 11, 2,  -3, \
+  -2, -2, -2, -3, -2, -1, -2, -3, 2, -1, -1, -2, -1, 3,  -3, -2, -2, 2,  7,  -1, \
+  0, -3, -3, -3, -1, -2, -2, -3, -3, 3, 1,  -2, 1,  -1, -2, -2, 0,  -3, -1, 4
+static __constant__ int8_t kBlosum62Dev[400] = {SSEQS_BLOSUM62_VALUES};
+static constexpr int8_t kBlosum62Host[400] = {SSEQS_BLOSUM62_VALUES};
+
 __host__ __device__ inline int8_t blosum62(int a, int b) {
-  constexpr int8_t M[400] = {
-      4, -1, -2, -2, 0,  -1, -1, 0,  -2, -1, -1, -1, -1, -2, -1, 1,  0,  -3, -2, 0,
-      -1, 5, 0,  -2, -3, 1,  0,  -2, 0,  -3, -2, 2,  -1, -3, -2, -1, -1, -3, -2, -3,
-      -2, 0, 6,  1,  -3, 0,  0,  0,  1,  -3, -3, 0,  -2, -3, -2, 1,  0,  -4, -2, -3,
-      -2, -2, 1, 6,  -3, 0,  2,  -1, -1, -3, -4, -1, -3, -3, -1, 0,  -1, -4, -3, -3,
-      0, -3, -3, -3, 9,  -3, -4, -3, -3, -1, -1, -3, -1, -2, -3, -1, -1, -2, -2, -1,
-      -1, 1, 0,  0,  -3, 5,  2,  -2, 0,  -3, -2, 1,  0,  -3, -1, 0,  -1, -2, -1, -2,
-      -1, 0, 0,  2,  -4, 2,  5,  -2, 0,  -3, -3, 1,  -2, -3, -1, 0,  -1, -3, -2, -2,
-      0, -2, 0,  -1, -3, -2, -2, 6,  -2, -4, -4, -2, -3, -3, -2, 0,  -2, -2, -3, -3,
-      -2, 0, 1,  -1, -3, 0,  0,  -2, 8,  -3, -3, -1, -2, -1, -2, -1, -2, -2, 2,  -3,
-      -1, -3, -3, -3, -1, -3, -3, -4, -3, 4, 2,  -3, 1,  0,  -3, -2, -1, -3, -1, 3,
-      -1, -2, -3, -4, -1, -2, -3, -4, -3, 2, 4,  -2, 2,  0,  -3, -2, -1, -2, -1, 1,
-      -1, 2, 0,  -1, -3, 1,  1,  -2, -1, -3, -2, 5,  -1, -3, -1, 0,  -1, -3, -2, -2,
-      -1, -1, -2, -3, -1, 0, -2, -3, -2, 1,  2,  -1, 5,  0,  -2, -1, -1, -1, -1, 1,
-      -2, -3, -3, -3, -2, -3, -3, -3, -1, 0, 0,  -3, 0,  6,  -4, -2, -2, 1,  3,  -1,
-      -1, -2, -2, -1, -3, -1, -1, -2, -2, -3, -3, -1, -2, -4, 7, -1, -1, -4, -3, -2,
-      1, -1, 1,  0,  -1, 0,  0,  0,  -1, -2, -2, 0,  -1, -2, -1, 4,  1,  -3, -2, -2,
-      0, -1, 0,  -1, -1, -1, -1, -2, -2, -1, -1, -1, -1, -2, -1, 1,  5,  -2, -2, 0,
-      -3, -3, -4, -4, -2, -2, -3, -2, -2, -3, -2, -3, -1, 1, -4, -3, -2, 11, 2,  -3,
-      -2, -2, -2, -3, -2, -1, -2, -3, 2, -1, -1, -2, -1, 3,  -3, -2, -2, 2,  7,  -1,
-      0, -3, -3, -3, -1, -2, -2, -3, -3, 3, 1,  -2, 1,  -1, -2, -2, 0,  -3, -1, 4};
-  return M[a * 20 + b];
+#ifdef __CUDA_ARCH__
+  return kBlosum62Dev[a * 20 + b];
+#else
+  return kBlosum62Host[a * 20 + b];
+#endif
 }
 
 // ASCII byte -> residue class (0..19, else 20).  Bytes >= 128 are class 20;

@@ -97,7 +97,26 @@ Cache& cache() {
   return c;
 }
 
-int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
+// Target counters of the streaming kernel: every launch takes the next slot
+// of this ring and zeroes it on its stream first, so launches in flight at
+// the same time (up to kTicketSlots of them) never share a counter.
+constexpr int kTicketSlots = 1024;
+static __device__ unsigned int g_sw_tickets[kTicketSlots];
+
+unsigned int* ticket_slot(int dev) {
+  static std::mutex mu;
+  static unsigned int* base[64] = {};
+  static unsigned next[64] = {};
+  std::lock_guard<std::mutex> lk(mu);
+  if (!base[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_sw_tickets) != cudaSuccess || !p) return nullptr;
+    base[dev] = static_cast<unsigned int*>(p);
+  }
+  return base[dev] + (next[dev]++ % kTicketSlots);
+}
+
+int launch_stream(SwArgs a, bool aff, cudaStream_t stream) {
   const int tpt = (a.Lq + 31) / 32;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
@@ -113,7 +132,7 @@ int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
                                (int)kp->smem) != cudaSuccess)
         return SSEQS_ERR_CUDA;
       int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kp->fn, kThreads,
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)kp->fn, kp->threads,
                                                         kp->smem) != cudaSuccess || nb < 1)
         return SSEQS_ERR_CUDA;
       mb = nb;
@@ -122,10 +141,25 @@ int launch_stream(const SwArgs& a, bool aff, cudaStream_t stream) {
   }
   const KernelInfo& k = *kp;
   const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
-  const int64_t need = (a.n + k.groups_per_block - 1) / k.groups_per_block;
-  const int grid = (int)std::max<int64_t>(1, std::min(full, need));
-  { k.fn<<<grid, kThreads, k.smem, stream>>>(a); count_launches(1); }
-  return status_of(cudaGetLastError());
+  // The kernel counts targets in 32 bits: launches take at most 2^30 each.
+  constexpr int64_t kPiece = int64_t(1) << 30;
+  for (int64_t t0 = 0; t0 < a.n; t0 += kPiece) {
+    SwArgs p = a;
+    p.n = std::min(kPiece, a.n - t0);
+    p.out = a.out + t0;
+    if (a.idx) p.idx = a.idx + t0;
+    else p.g0 = (int32_t)(a.g0 + t0);
+    p.ticket = ticket_slot(dev);
+    if (!p.ticket) return SSEQS_ERR_CUDA;
+    if (cudaMemsetAsync(p.ticket, 0, sizeof(unsigned int), stream) != cudaSuccess)
+      return SSEQS_ERR_CUDA;
+    const int64_t need = (p.n + k.groups_per_block - 1) / k.groups_per_block;
+    const int grid = (int)std::max<int64_t>(1, std::min(full, need));
+    { k.fn<<<grid, k.threads, k.smem, stream>>>(p); count_launches(1); }
+    const int st = status_of(cudaGetLastError());
+    if (st != SSEQS_OK) return st;
+  }
+  return SSEQS_OK;
 }
 
 int run(bool aff, SwArgs a, cudaStream_t stream) {

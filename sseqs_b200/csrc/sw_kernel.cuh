@@ -33,11 +33,14 @@
 // padding words (-32768 + open, or -16384) keep every intermediate inside
 // int16 and can never raise a score.
 //
-// Targets are streamed: each lane group walks a contiguous range of targets
-// four rows at a time, the four bytes of the next quad prefetched with two
-// aligned 32-bit loads; when a target ends (rows past its end are padding
-// rows) the group writes its score, resets its state and moves on while the
-// other groups of the warp keep going.
+// Targets are streamed: each lane group takes targets from a launch-wide
+// counter (a few at a time, the next grab issued one chunk ahead so its
+// latency is hidden), which keeps every group busy until the last targets
+// whatever their lengths.  A target is read four rows at a time, the four
+// bytes of the next quad prefetched with two aligned 32-bit loads; when a
+// target ends (rows past its end are padding rows) the group writes its
+// score, resets its state and moves on while the other groups of the warp
+// keep going.
 #pragma once
 #include <algorithm>
 #include <utility>
@@ -48,7 +51,6 @@ namespace sseqs {
 namespace sw {
 
 constexpr int kMaxQuery = 2048;
-constexpr int kThreads = 128;
 
 struct SwArgs {
   const uint8_t* q;       // query residue classes
@@ -61,12 +63,15 @@ struct SwArgs {
   int skip;               // bytes not scored at the start of every window
   int32_t* out;
   int p0, p1;             // linear: gap; affine: open, extend
+  unsigned int* ticket;   // zeroed launch-wide target counter (fast kernel)
 };
 
 // Window of one target (sseqs/sw.cu:66-77): rows [pos, end), or no rows and
 // an immediate result (-1 for an empty or inverted window, 0 otherwise).
+// Window bounds come from int32 delimiter positions, so rows with bytes lie
+// in [0, 2^31) and fit 32-bit arithmetic.
 struct Win {
-  int64_t pos, end;
+  uint32_t pos, end;
   int32_t res;
   bool rows;
 };
@@ -75,14 +80,15 @@ __device__ __forceinline__ Win window_of(const SwArgs& a, int64_t t) {
   const int32_t g = a.idx ? a.idx[t] : (int32_t)(a.g0 + t);
   const int64_t base = (g == 0) ? -1 : (int64_t)a.starts[g - 1];
   const int64_t len = (int64_t)a.starts[g] - base - 1;
+  const int64_t pos = base + 1 + a.skip, end = base + 1 + len;
   Win w;
-  w.pos = base + 1 + a.skip;
-  w.end = base + 1 + len;
+  w.pos = (uint32_t)pos;
+  w.end = (uint32_t)end;
   if (len == 0 || len < -1) {
     w.rows = false;
     w.res = -1;
   } else {
-    w.rows = w.pos < w.end;
+    w.rows = pos < end;
     w.res = 0;
   }
   return w;
@@ -116,8 +122,23 @@ struct Layout {
   static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
 };
 
+// Block shape per instantiation.  The state of a lane is about NWD words
+// (linear: H; affine: D and Iy) plus its profile row, so registers grow
+// with NWD.  Up to ~128 registers a block has 8 warps that share one copy
+// of the query profile in shared memory, with the register cap set for 3
+// blocks (85 registers) or 2 (128) per SM; larger states use blocks of 4
+// warps, which pack the register file more finely.
 template <int TPT, int W, bool AFF>
-__global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
+struct Shape {
+  static constexpr int NWD = W * TPT;
+  static constexpr int est_regs = AFF ? 3 * NWD + 32 : 2 * NWD + 51;
+  static constexpr int threads = est_regs <= 128 ? 256 : 128;
+  static constexpr int min_blocks = threads == 256 ? (est_regs <= 85 ? 3 : 2) : 1;
+};
+
+template <int TPT, int W, bool AFF>
+__global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF>::min_blocks)
+    sw_stream_kernel(SwArgs a) {
   using L = Layout<TPT, W>;
   constexpr int G = L::G;
   extern __shared__ uint4 smem4[];
@@ -149,16 +170,11 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
   const int grp = lane / G;
   const int gl = lane - grp * G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
-  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t ngroups = nwarps * L::GPW;
-  const int64_t gid = wid * L::GPW + grp;
-  int64_t t = (a.n * gid) / ngroups;
-  const int64_t t_hi = (a.n * (gid + 1)) / ngroups;
+  const int leader = grp * G;
 
-  const uint32_t gap2 = pack2(a.p0, a.p0);    // linear gap, -16384 <= gap <= 0
-  const uint32_t open2 = pack2(a.p0, a.p0);   // affine open, 0 <= open <= 16384
-  const uint32_t next2 = pack2(-a.p1, -a.p1); // affine -extend, 0 <= extend <= 16384
+  const uint32_t gap2 = pack2(a.p0, a.p0);     // linear gap, -16384 <= gap <= 0
+  const uint32_t nopen2 = pack2(-a.p0, -a.p0); // affine -open, 0 <= open <= 16384
+  const uint32_t next2 = pack2(-a.p1, -a.p1);  // affine -extend, 0 <= extend <= 16384
   // state at row -1: H = 0 (linear state is H + gap), D = Iy = 0 (affine)
   const uint32_t init = AFF ? 0u : gap2;
 
@@ -201,6 +217,15 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
         // (Hg_left = gap at the first column of a stripe).  The next
         // column's diagonal sum is formed before S[k] is overwritten, so the
         // new value can take the old one's register.
+        //
+        // The running maximum is taken over the diagonal sums u rather than
+        // over H: with gap <= 0 a cell whose H comes from Hg_up or Hg_left is
+        // never above the cell it came from, so following those moves back
+        // ends at a cell whose H is its u (or 0), and max H = max(0, max u).
+        // (Padding u lie 16384 below a real cell and never win.)  Taking
+        // the maximum over u keeps u a value of its own, so the compiler
+        // leaves its add on the FMA pipe instead of folding it into an
+        // add-max on the ALU pipe, which is the busier one.
         uint32_t hg_left = 0;
         uint32_t u = __vadd2(diag, s[w * TPT]);                             // FMA pipe
 #pragma unroll
@@ -211,9 +236,9 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
                                       : __vimax3_s16x2_relu(u, up, hg_left); // ALU pipe
           hg_left = __vadd2(h, gap2);                                       // FMA pipe
           S[w][k] = hg_left;
+          if (((w * TPT + k) & 1) == 0) pend = u;
+          else best = __vimax3_s16x2(best, pend, u);
           u = u_next;
-          if (((w * TPT + k) & 1) == 0) pend = h;
-          else best = __vimax3_s16x2(best, pend, h);
         }
       } else {
         // M' = D_diag + s (unclamped), Mo = M' - open          FMA pipe
@@ -224,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
         uint32_t mp = __vadd2(diag, s[w * TPT]);
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
-          const uint32_t mo = __vsub2(mp, open2);
+          const uint32_t mo = __vadd2(mp, nopen2);
           const uint32_t mp_next = (k + 1 < TPT) ? __vadd2(S[w][k], s[w * TPT + k + 1]) : 0u;
           if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
           const uint32_t y = Y[w][k];
@@ -246,41 +271,67 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
   // no load leaves the windows' own 4-byte words.
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
-  const int64_t aoff = (int64_t)(au & 3);
+  const uint32_t aoff = (uint32_t)(au & 3);
   struct Quad { uint32_t w0, w1; };
-  auto fetch = [&](int64_t p, int64_t e) -> Quad {
-    const int64_t ap = p + aoff;
-    const int64_t wi = ap >> 2;
+  auto fetch = [&](uint32_t p, uint32_t e) -> Quad {
+    const uint32_t wi = (p + aoff) >> 2;
     Quad q;
     q.w0 = __ldg(abase + wi);
     q.w1 = ((wi + 1) << 2) < e + aoff ? __ldg(abase + wi + 1) : 0u;
     return q;
   };
   uint32_t c0 = kClsPad, c1 = kClsPad, c2 = kClsPad, c3 = kClsPad;
-  auto classes = [&](const Quad& q, int64_t p, int64_t e) {
-    const uint32_t raw = __funnelshift_r(q.w0, q.w1, (uint32_t)((p + aoff) & 3) * 8u);
+  auto classes = [&](const Quad& q, uint32_t p, uint32_t e) {
+    const uint32_t raw = __funnelshift_r(q.w0, q.w1, ((p + aoff) & 3u) * 8u);
     c0 = p + 0 < e ? lut[raw & 0xffu] : kClsPad;
     c1 = p + 1 < e ? lut[(raw >> 8) & 0xffu] : kClsPad;
     c2 = p + 2 < e ? lut[(raw >> 16) & 0xffu] : kClsPad;
     c3 = p + 3 < e ? lut[raw >> 24] : kClsPad;
   };
 
-  // ---- target bookkeeping (group-uniform) ----
-  Win cur, nxt;
-  bool active = false, nxt_ok = false;
-  auto start_from = [&](int64_t tt) {   // first target at or after tt with rows
-    active = false;
-    nxt_ok = false;
-    t = tt;
-    while (t < t_hi) {
-      cur = window_of(a, t);
-      if (cur.rows) { active = true; break; }
-      if (gl == 0) a.out[t] = cur.res;
-      ++t;
-    }
-    if (active && t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
+  // ---- target order (group-uniform).  The group leader takes CH targets
+  // at a time from the launch-wide counter; the grab for the chunk after
+  // the current one is issued when the current one is taken, and its value
+  // is broadcast to the group only when that chunk is reached.
+  // The host splits launches so that n < 2^30: target indices and the
+  // counter (which overshoots n by at most two grabs per group) fit 32 bits.
+  constexpr int CH = (64 / TPT) > 1 ? 64 / TPT : 1;
+  const int n = (int)a.n;
+  unsigned pre_raw = 0;   // leader only: start of the prefetched chunk
+  auto issue_grab = [&]() {
+    if (gl == 0) pre_raw = atomicAdd(a.ticket, (unsigned)CH);
   };
-  start_from(t);
+  int c_hi;               // end of the chunk the sequence is in
+  auto take_chunk = [&]() -> int {
+    const int c = (int)__shfl_sync(gmask, pre_raw, leader);
+    c_hi = c < n - CH ? c + CH : n;
+    if (c < n) issue_grab();
+    return c;
+  };
+  auto successor = [&](int x) -> int {   // next target after x (>= n: none)
+    return x + 1 < c_hi ? x + 1 : take_chunk();
+  };
+
+  Win cur, nxt;
+  int t, tn = 0;
+  bool active = false, nxt_ok = false;
+  auto start_at = [&](int tt) {   // first target with rows at or after tt
+    t = tt;
+    while (t < n) {
+      cur = window_of(a, t);
+      if (cur.rows) break;
+      if (gl == 0) a.out[t] = cur.res;
+      t = successor(t);
+    }
+    active = t < n;
+    nxt_ok = false;
+    if (active) {
+      tn = successor(t);
+      if (tn < n) { nxt = window_of(a, tn); nxt_ok = true; }
+    }
+  };
+  issue_grab();
+  start_at(take_chunk());
   if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
 
   while (__any_sync(0xffffffffu, active)) {
@@ -305,13 +356,14 @@ __global__ void __launch_bounds__(kThreads) sw_stream_kernel(SwArgs a) {
         if (gl == 0) a.out[t] = v;
         reset();
         if (pf_nxt) {
-          ++t;
+          t = tn;
           cur = nxt;
-          nxt_ok = false;
-          if (t + 1 < t_hi) { nxt = window_of(a, t + 1); nxt_ok = true; }
+          tn = successor(t);
+          nxt_ok = tn < n;
+          if (nxt_ok) nxt = window_of(a, tn);
           classes(pf, cur.pos, cur.end);
         } else {
-          start_from(t + 1);
+          start_at(tn);
           if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
           else c0 = c1 = c2 = c3 = kClsPad;
         }
@@ -328,6 +380,7 @@ using KernelFn = void (*)(SwArgs);
 struct KernelInfo {
   KernelFn fn = nullptr;
   size_t smem = 0;
+  int threads = 0;
   int groups_per_block = 0;
   int words = 0;
 };
@@ -338,7 +391,8 @@ KernelInfo make_info() {
   KernelInfo k;
   k.fn = sw_stream_kernel<TPT, W, AFF>;
   k.smem = Layout<TPT, W>::smem;
-  k.groups_per_block = (kThreads / 32) * Layout<TPT, W>::GPW;
+  k.threads = Shape<TPT, W, AFF>::threads;
+  k.groups_per_block = (k.threads / 32) * Layout<TPT, W>::GPW;
   k.words = W;
   return k;
 }
