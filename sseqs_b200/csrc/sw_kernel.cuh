@@ -36,11 +36,11 @@
 // Targets are streamed: each lane group takes targets from a launch-wide
 // counter (a few at a time, the next grab issued one chunk ahead so its
 // latency is hidden), which keeps every group busy until the last targets
-// whatever their lengths.  A target is read four rows at a time, the four
-// bytes of the next quad prefetched with two aligned 32-bit loads; when a
-// target ends (rows past its end are padding rows) the group writes its
-// score, resets its state and moves on while the other groups of the warp
-// keep going.
+// whatever their lengths.  A target is read R rows at a time (4 linear, 8
+// affine), the R bytes of the next step prefetched with R/4 + 1 aligned
+// 32-bit loads; when a target ends (rows past its end are padding rows) the
+// group writes its score, resets its state and moves on while the other
+// groups of the warp keep going.
 #pragma once
 #include <algorithm>
 #include <utility>
@@ -51,6 +51,12 @@ namespace sseqs {
 namespace sw {
 
 constexpr int kMaxQuery = 2048;
+// Target rows per byte fetch: the per-fetch bookkeeping is shared by this
+// many rows, and a target's last fetch pads with up to R-1 rows.  The affine
+// kernel takes 8 (measured 10% faster than 4 at query length 858); the
+// linear kernel keeps 4, where 8 gained nothing and made the compiler spill.
+template <bool AFF>
+__host__ __device__ constexpr int rows_per_fetch() { return AFF ? 8 : 4; }
 
 struct SwArgs {
   const uint8_t* q;       // query residue classes
@@ -131,7 +137,7 @@ struct Layout {
 template <int TPT, int W, bool AFF>
 struct Shape {
   static constexpr int NWD = W * TPT;
-  static constexpr int est_regs = AFF ? 3 * NWD + 32 : 2 * NWD + 51;
+  static constexpr int est_regs = AFF ? 3 * NWD + 32 : 2 * NWD + 53;
   static constexpr int threads = est_regs <= 128 ? 256 : 128;
   static constexpr int min_blocks = threads == 256 ? (est_regs <= 85 ? 3 : 2) : 1;
 };
@@ -266,27 +272,42 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
     if ((L::NWD & 1) != 0) best = __vimax_s16x2_relu(best, pend);
   };
 
-  // ---- target bytes: four rows at a time from two aligned 32-bit words.
+  // ---- target bytes: R rows at a time from R/4 + 1 aligned 32-bit words.
   // A word is loaded only when it holds a byte of the window being read, so
   // no load leaves the windows' own 4-byte words.
+  constexpr int R = rows_per_fetch<AFF>();
+  constexpr int NWORDS = R / 4 + 1;
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
   const uint32_t aoff = (uint32_t)(au & 3);
-  struct Quad { uint32_t w0, w1; };
-  auto fetch = [&](uint32_t p, uint32_t e) -> Quad {
+  struct Bytes { uint32_t w[NWORDS]; };
+  auto fetch = [&](uint32_t p, uint32_t e) -> Bytes {   // needs p < e
     const uint32_t wi = (p + aoff) >> 2;
-    Quad q;
-    q.w0 = __ldg(abase + wi);
-    q.w1 = ((wi + 1) << 2) < e + aoff ? __ldg(abase + wi + 1) : 0u;
+    Bytes q;
+    q.w[0] = __ldg(abase + wi);
+#pragma unroll
+    for (int k = 1; k < NWORDS; ++k)
+      q.w[k] = ((wi + k) << 2) < e + aoff ? __ldg(abase + wi + k) : 0u;
     return q;
   };
-  uint32_t c0 = kClsPad, c1 = kClsPad, c2 = kClsPad, c3 = kClsPad;
-  auto classes = [&](const Quad& q, uint32_t p, uint32_t e) {
-    const uint32_t raw = __funnelshift_r(q.w0, q.w1, ((p + aoff) & 3u) * 8u);
-    c0 = p + 0 < e ? lut[raw & 0xffu] : kClsPad;
-    c1 = p + 1 < e ? lut[(raw >> 8) & 0xffu] : kClsPad;
-    c2 = p + 2 < e ? lut[(raw >> 16) & 0xffu] : kClsPad;
-    c3 = p + 3 < e ? lut[raw >> 24] : kClsPad;
+  // residue classes of the next R rows, four 8-bit classes per word
+  constexpr uint32_t kPadWord = kClsPad * 0x01010101u;
+  uint32_t cw[R / 4];
+#pragma unroll
+  for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
+  auto classes = [&](const Bytes& q, uint32_t p, uint32_t e) {
+    const uint32_t sh = ((p + aoff) & 3u) * 8u;
+#pragma unroll
+    for (int h = 0; h < R / 4; ++h) {
+      const uint32_t raw = __funnelshift_r(q.w[h], q.w[h + 1], sh);
+      uint32_t word = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const uint32_t cl = p + (4 * h + b) < e ? lut[(raw >> (8 * b)) & 0xffu] : kClsPad;
+        word |= cl << (8 * b);
+      }
+      cw[h] = word;
+    }
   };
 
   // ---- target order (group-uniform).  The group leader takes CH targets
@@ -335,19 +356,17 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
   if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
 
   while (__any_sync(0xffffffffu, active)) {
-    // prefetch the bytes of the next quad of this group
-    Quad pf{0u, 0u};
+    // prefetch the bytes of the next R rows of this group
+    Bytes pf{};
     bool pf_nxt = false;
     if (active) {
-      if (cur.pos + 4 < cur.end) pf = fetch(cur.pos + 4, cur.end);
+      if (cur.pos + R < cur.end) pf = fetch(cur.pos + R, cur.end);
       else if (nxt_ok && nxt.rows) { pf = fetch(nxt.pos, nxt.end); pf_nxt = true; }
     }
-    row(c0);
-    row(c1);
-    row(c2);
-    row(c3);
+#pragma unroll
+    for (int r = 0; r < R; ++r) row((int)((cw[r / 4] >> (8 * (r % 4))) & 0xffu));
     if (active) {
-      cur.pos += 4;
+      cur.pos += R;
       if (cur.pos >= cur.end) {
         // target finished (rows past its end were padding rows)
         int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
@@ -364,8 +383,12 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
           classes(pf, cur.pos, cur.end);
         } else {
           start_at(tn);
-          if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
-          else c0 = c1 = c2 = c3 = kClsPad;
+          if (active) {
+            classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
+          } else {
+#pragma unroll
+            for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
+          }
         }
       } else {
         classes(pf, cur.pos, cur.end);
