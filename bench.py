@@ -189,6 +189,74 @@ def prefiltered_leg(M, db, queries, exact_rows, per_query=32768):
             "queries": len(queries)}
 
 
+def batched_leg(db, n_queries, seed=3):
+    """Batched uneven queries: lengths log-normal (median 300, sigma 0.6)
+    clipped to 16..2048, affine 11/1 over every segment of the resident
+    database, top-4096 per query.  Times the bucketed, graph-replayed path
+    (``batched.BatchedSearcher``; its first call captures the graphs) against
+    the same work one query at a time (``sw.sw_scan`` + top-k per batch), and
+    checks that both give identical hit lists."""
+    import torch
+    from sseqs_b200 import batched, dbtools, select
+    sw = importlib.import_module("sseqs_b200.sw")
+    rng = np.random.default_rng(seed)
+    lengths = np.clip(np.round(np.exp(rng.normal(np.log(300), 0.6, n_queries))), 16, 2048)
+    queries = [dbtools.random_query(int(L), 5000 + i) for i, L in enumerate(lengths)]
+    rows_aff = 0
+    for b in db.batches:
+        if b.n_segments > 2:
+            ln = b.lengths[1:b.n_segments - 1].to(torch.int64)
+            rows_aff += int((ln - 1).clamp_(min=0).sum().item())
+    cells = int(sum(int(L) for L in lengths)) * rows_aff
+    searcher = batched.BatchedSearcher(db, top_k=TOP_K)
+    searcher.search(queries)                         # autotune + graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    got = searcher.search(queries)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+
+    def one(q):
+        enc = sw.encode_query(q)
+        rows = []
+        for bi, b in enumerate(db.batches):
+            n = b.n_segments - 2
+            if n <= 0:
+                continue
+            s = sw.sw_scan(enc, b.ascii, b.delim, affine=True, g0=1, n_targets=n, skip=1,
+                           gap_a=11, gap_b=1)
+            p = select.topk_indices(s, min(TOP_K, n)).long()
+            rows.append((s[p], bi, p + 1))
+        return rows
+
+    one(queries[0])
+    torch.cuda.synchronize()
+    e0.record()
+    ref = [one(q) for q in queries]
+    e1.record()
+    torch.cuda.synchronize()
+    ms_q = e0.elapsed_time(e1)
+    same = True
+    for h, rows in zip(got, ref):
+        sc = np.concatenate([r[0].cpu().numpy() for r in rows])
+        bt = np.concatenate([np.full(r[0].numel(), r[1], np.int32) for r in rows])
+        sg = np.concatenate([r[2].cpu().numpy() for r in rows])
+        o = np.lexsort((sg, bt, -sc.astype(np.int64)))[:TOP_K]
+        same &= (np.array_equal(h.scores, sc[o]) and np.array_equal(h.batch, bt[o])
+                 and np.array_equal(h.segment, sg[o]))
+    return {"queries": n_queries,
+            "lengths": "log-normal median 300 sigma 0.6, clipped 16..2048, seed %d" % seed,
+            "length_range": [int(lengths.min()), int(lengths.max())],
+            "buckets": len(batched.buckets([int(L) for L in lengths])),
+            "graphs": len(searcher.plans),
+            "gcups_batched": round(cells / (ms_b * 1e-3) / 1e9, 1),
+            "gcups_one_query_at_a_time": round(cells / (ms_q * 1e-3) / 1e9, 1),
+            "ms_batched": round(ms_b, 1), "ms_one_query_at_a_time": round(ms_q, 1),
+            "cells": cells, "identical_hits": bool(same)}
+
+
 def measured_peak(name):
     """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
     int pipes), in int16x2 lane-instructions per second."""
@@ -389,6 +457,8 @@ def bench_b200(args):
     }
     if world == 1 and args.prefilter_steps > 0:
         out["prefiltered"] = prefiltered_leg(M, db, timed[:args.prefilter_steps], exact_rows)
+    if world == 1 and args.batched_queries > 0:
+        out["batched"] = batched_leg(db, args.batched_queries)
     if world == 1 and not args.no_cpu_baseline:
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
@@ -451,6 +521,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--prefilter-steps", type=int, default=4,
                     help="queries of the prefiltered (FFT) leg; 0 skips it")
+    ap.add_argument("--batched-queries", type=int, default=16,
+                    help="queries of the batched uneven-length leg; 0 skips it")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -98,6 +98,30 @@ int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
                   const uint8_t* ascii, const int32_t* delim, int skip,
                   int32_t* out, int gap_a, int gap_b, cudaStream_t stream);
 
+/* sseqs_sw_scan for several queries of one stripe width against one batch,
+ * in one launch per 128 queries (the batched path; the reference runs one
+ * query at a time, sseqs/msa.py:235).  Query i has query_lens[i] (device
+ * int32) residue classes at queries + i * query_stride (device), scores the
+ * targets of sseqs_sw_scan -- with good_idx + i * idx_stride as its list
+ * when good_idx is given (idx_stride 0: one list for all, else >=
+ * n_targets) -- and writes its scores to out + i * out_stride (out_stride
+ * >= n_targets).  Every length
+ * must satisfy ceil(len/32) == tpt and len <= query_stride; a query that does
+ * not is not scored and its row is filled with INT32_MIN.  tickets: device
+ * scratch of n_queries uint32 (target counters, zeroed by the call on
+ * `stream`).  Gap parameters must lie in the int16 domain (linear -16384 <=
+ * gap <= 0; affine 0 <= open, extend <= 16384), else SSEQS_ERR_UNSUPPORTED.
+ * Every query's scores are identical to its own sseqs_sw_scan call.  The
+ * lengths are read on the device, so a captured CUDA graph can be replayed
+ * with other queries of the same width. */
+int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const uint8_t* queries,
+                          int64_t query_stride, const int32_t* query_lens,
+                          const int32_t* good_idx, int64_t idx_stride, int32_t g0,
+                          int64_t n_targets,
+                          const uint8_t* ascii, const int32_t* delim, int skip,
+                          int32_t* out, int64_t out_stride, int gap_a, int gap_b,
+                          uint32_t* tickets, cudaStream_t stream);
+
 /* ------------------------------------------------------------ selection */
 /* Positions (int32, increasing) of every '@' (64) byte of a decoded batch:
  * replaces `delim_pos = arange[ascii == 64]` (sseqs/msa.py:227).  Writes at

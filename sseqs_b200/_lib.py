@@ -31,6 +31,8 @@ _SIGNATURES = {
     "sseqs_sw_linear": (_I, [_P, _I, _P, _P, _P, _I64, _P, _I, _P]),
     "sseqs_sw_affine": (_I, [_P, _I, _P, _P, _P, _I64, _P, _I, _I, _P]),
     "sseqs_sw_scan": (_I, [_I, _P, _I, _P, ctypes.c_int32, _I64, _P, _P, _I, _P, _I, _I, _P]),
+    "sseqs_sw_scan_queries": (_I, [_I, _I, _I, _P, _I64, _P, _P, _I64, ctypes.c_int32, _I64,
+                                   _P, _P, _I, _P, _I64, _I, _I, _P, _P]),
     "sseqs_find_delims_workspace_bytes": (_SZ, [_I64]),
     "sseqs_find_delims": (_I, [_P, _I64, _P, _I64, _P, _P, _SZ, _P]),
     "sseqs_segment_table_workspace_bytes": (_SZ, [_I64]),

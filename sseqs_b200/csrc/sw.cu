@@ -1,6 +1,7 @@
 // Score-only Smith-Waterman: dispatch, the exact fallback kernel and the C
 // ABI.  The fast int16x2 kernel is the template in sw_kernel.cuh (see there
 // for its design), instantiated per stripe width in sw_inst_*.cu.
+#include <climits>
 #include <mutex>
 
 #include "sw_kernel.cuh"
@@ -116,7 +117,10 @@ unsigned int* ticket_slot(int dev) {
   return base[dev] + (next[dev]++ % kTicketSlots);
 }
 
-int launch_stream(SwArgs a, bool aff, cudaStream_t stream) {
+// Launches the streaming kernel for one query (qt == nullptr; target
+// counter from the ring) or for the qt->n queries of a table (counters
+// a.ticket[0 .. qt->n), provided by the caller).
+int launch_stream(SwArgs a, bool aff, const QueryTable* qt, cudaStream_t stream) {
   const int tpt = (a.Lq + 31) / 32;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
@@ -141,6 +145,10 @@ int launch_stream(SwArgs a, bool aff, cudaStream_t stream) {
   }
   const KernelInfo& k = *kp;
   const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
+  QueryTable none{};
+  const QueryTable& table = qt ? *qt : none;
+  const int ny = qt ? qt->n : 1;
+  unsigned int* const tickets = a.ticket;
   // The kernel counts targets in 32 bits: launches take at most 2^30 each.
   constexpr int64_t kPiece = int64_t(1) << 30;
   for (int64_t t0 = 0; t0 < a.n; t0 += kPiece) {
@@ -149,17 +157,24 @@ int launch_stream(SwArgs a, bool aff, cudaStream_t stream) {
     p.out = a.out + t0;
     if (a.idx) p.idx = a.idx + t0;
     else p.g0 = (int32_t)(a.g0 + t0);
-    p.ticket = ticket_slot(dev);
+    p.ticket = qt ? tickets : ticket_slot(dev);
     if (!p.ticket) return SSEQS_ERR_CUDA;
-    if (cudaMemsetAsync(p.ticket, 0, sizeof(unsigned int), stream) != cudaSuccess)
+    if (cudaMemsetAsync(p.ticket, 0, sizeof(unsigned int) * ny, stream) != cudaSuccess)
       return SSEQS_ERR_CUDA;
     const int64_t need = (p.n + k.groups_per_block - 1) / k.groups_per_block;
     const int grid = (int)std::max<int64_t>(1, std::min(full, need));
-    { k.fn<<<grid, k.threads, k.smem, stream>>>(p); count_launches(1); }
+    { k.fn<<<dim3(grid, ny), k.threads, k.smem, stream>>>(p, table); count_launches(1); }
     const int st = status_of(cudaGetLastError());
     if (st != SSEQS_OK) return st;
   }
   return SSEQS_OK;
+}
+
+bool fast_domain(bool aff, int p0, int p1) {
+  // The int16x2 kernel needs every intermediate inside int16: cells are in
+  // [0, 11*2048], profile words s - open in [-16388, 11].
+  return aff ? (p0 >= 0 && p0 <= 16384 && p1 >= 0 && p1 <= 16384)
+             : (p0 <= 0 && p0 >= -16384);
 }
 
 int run(bool aff, SwArgs a, cudaStream_t stream) {
@@ -173,11 +188,7 @@ int run(bool aff, SwArgs a, cudaStream_t stream) {
     return status_of(cudaGetLastError());
   }
   if (!a.q) return SSEQS_ERR_ARG;
-  // The int16x2 kernel needs every intermediate inside int16: cells are in
-  // [0, 11*2048], profile words s - open in [-16388, 11].
-  const bool fast = aff ? (a.p0 >= 0 && a.p0 <= 16384 && a.p1 >= 0 && a.p1 <= 16384)
-                        : (a.p0 <= 0 && a.p0 >= -16384);
-  if (fast) return launch_stream(a, aff, stream);
+  if (fast_domain(aff, a.p0, a.p1)) return launch_stream(a, aff, nullptr, stream);
   if (a.skip != 0) return SSEQS_ERR_UNSUPPORTED;
   const int grid = (int)std::min<int64_t>((a.n + 127) / 128, (int64_t)device_sm_count() * 4);
   { sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0); count_launches(1); }
@@ -280,6 +291,39 @@ extern "C" int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len
   if (skip < 0 || g0 < 0) return SSEQS_ERR_ARG;
   SwArgs a{query_idx, query_len, good_idx, g0, n_targets, ascii, delim, skip, out, gap_a, gap_b};
   return run(affine != 0, a, stream);
+}
+
+extern "C" int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const uint8_t* queries,
+                                     int64_t query_stride, const int32_t* query_lens,
+                                     const int32_t* good_idx, int64_t idx_stride, int32_t g0,
+                                     int64_t n_targets,
+                                     const uint8_t* ascii, const int32_t* delim, int skip,
+                                     int32_t* out, int64_t out_stride, int gap_a, int gap_b,
+                                     uint32_t* tickets, cudaStream_t stream) {
+  if (n_queries < 0 || skip < 0 || g0 < 0 || n_targets < 0 || idx_stride < 0)
+    return SSEQS_ERR_ARG;
+  if (good_idx && idx_stride > 0 && idx_stride < n_targets) return SSEQS_ERR_ARG;
+  if (n_queries == 0 || n_targets == 0) return SSEQS_OK;
+  if (!queries || !query_lens || !tickets || !out || !ascii || !delim ||
+      out_stride < n_targets || query_stride < 1 || query_stride > INT32_MAX)
+    return SSEQS_ERR_ARG;
+  if (tpt < 1 || tpt > kMaxQuery / 32) return SSEQS_ERR_UNSUPPORTED;
+  const bool aff = affine != 0;
+  if (!fast_domain(aff, gap_a, gap_b)) return SSEQS_ERR_UNSUPPORTED;
+  for (int q0 = 0; q0 < n_queries; q0 += kMaxLaunchQueries) {
+    QueryTable qt{};
+    qt.n = std::min(kMaxLaunchQueries, n_queries - q0);
+    qt.lens = query_lens + q0;
+    qt.q_stride = (int32_t)query_stride;
+    qt.out_stride = out_stride;
+    qt.idx_stride = good_idx ? idx_stride : 0;
+    const int32_t* idx0 = good_idx ? good_idx + q0 * qt.idx_stride : nullptr;
+    SwArgs a{queries + (size_t)q0 * query_stride, tpt * 32, idx0, g0, n_targets,
+             ascii, delim, skip, out + q0 * out_stride, gap_a, gap_b, tickets + q0};
+    const int st = launch_stream(a, aff, &qt, stream);
+    if (st != SSEQS_OK) return st;
+  }
+  return SSEQS_OK;
 }
 
 extern "C" int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream) {

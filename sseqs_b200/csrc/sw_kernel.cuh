@@ -72,6 +72,22 @@ struct SwArgs {
   unsigned int* ticket;   // zeroed launch-wide target counter (fast kernel)
 };
 
+// Several queries of the same stripe width in one launch: blockIdx.y picks
+// the query, which reads lens[y] (device) residues at q + y * q_stride,
+// scores the targets idx + y * idx_stride (when idx is given), writes its
+// scores at out + y * out_stride and takes targets from ticket[y].  n == 0
+// is the single-query launch (SwArgs alone).  A length
+// that does not belong to the launch's stripe width (or exceeds q_stride)
+// is not scored: its output row is filled with INT32_MIN.
+constexpr int kMaxLaunchQueries = 128;
+struct QueryTable {
+  const int32_t* lens;
+  int64_t out_stride;
+  int64_t idx_stride;
+  int32_t q_stride;
+  int32_t n;
+};
+
 // Window of one target (sseqs/sw.cu:66-77): rows [pos, end), or no rows and
 // an immediate result (-1 for an empty or inverted window, 0 otherwise).
 // Window bounds come from int32 delimiter positions, so rows with bytes lie
@@ -144,8 +160,23 @@ struct Shape {
 
 template <int TPT, int W, bool AFF>
 __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF>::min_blocks)
-    sw_stream_kernel(SwArgs a) {
+    sw_stream_kernel(SwArgs a, const QueryTable qt) {
   using L = Layout<TPT, W>;
+  if (qt.n > 0) {
+    const int y = blockIdx.y;
+    const int len = qt.lens[y];
+    a.q += (size_t)y * qt.q_stride;
+    a.out += (int64_t)y * qt.out_stride;
+    if (a.idx) a.idx += (int64_t)y * qt.idx_stride;
+    a.ticket += y;
+    if (len < 1 || (len + 31) / 32 != TPT || len > qt.q_stride) {
+      for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+           i += (int64_t)gridDim.x * blockDim.x)
+        a.out[i] = INT32_MIN;
+      return;
+    }
+    a.Lq = len;
+  }
   constexpr int G = L::G;
   extern __shared__ uint4 smem4[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);
@@ -398,7 +429,7 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
 }
 
 // ------------------------------------------------------------ registry
-using KernelFn = void (*)(SwArgs);
+using KernelFn = void (*)(SwArgs, const QueryTable);
 
 struct KernelInfo {
   KernelFn fn = nullptr;

@@ -1,0 +1,109 @@
+"""GPU tests of the batched path: many queries of one stripe width in one
+launch give exactly the scores of their single-query launches, and the
+bucketed, graph-replayed search gives exactly the per-query top-k."""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _db(n_seqs=3000, chunk_bytes=120_000, seed=3):
+    from sseqs_b200 import dbtools
+    from sseqs_b200.database import Database
+    q = dbtools.random_query(300, seed)
+    syn = dbtools.synthetic_db([q], n_seqs, 0.02, (0.3, 0.9), seed=seed, device="cpu",
+                               chunk_bytes=chunk_bytes)
+    return q, Database(syn.chunks, bs=chunk_bytes)
+
+
+def _pack(queries):
+    sw = importlib.import_module("sseqs_b200.sw")
+    enc = [sw.encode_query(q) for q in queries]
+    buf = torch.zeros((len(enc), 2048), dtype=torch.uint8, device="cuda")
+    for i, e in enumerate(enc):
+        buf[i, :e.numel()] = e
+    lens = torch.tensor([e.numel() for e in enc], dtype=torch.int32, device="cuda")
+    return enc, buf, lens
+
+
+@pytest.mark.parametrize("lengths", [[300, 289, 320, 300, 305], [40, 33, 64], [2048, 2017],
+                                     [7, 1, 32, 20]])
+@pytest.mark.parametrize("affine", [False, True])
+def test_scan_queries_equals_single_query_scans(lengths, affine):
+    from sseqs_b200 import batched, dbtools
+    sw = importlib.import_module("sseqs_b200.sw")
+    _, db = _db()
+    b = db.batches[0]
+    queries = [dbtools.random_query(L, 50 + i) for i, L in enumerate(lengths)]
+    enc, buf, lens = _pack(queries)
+    tpt = (lengths[0] + 31) // 32
+    kw = dict(affine=affine, skip=1 if affine else 0, gap_a=11 if affine else -1, gap_b=1)
+    n = b.n_segments - 2
+    got = batched.sw_scan_queries(buf, lens, tpt, b.ascii, b.delim, g0=1, n_targets=n, **kw)
+    # gathered targets too: every third segment, out of order
+    idx = torch.arange(n, 0, -3, dtype=torch.int32, device="cuda")
+    got_i = batched.sw_scan_queries(buf, lens, tpt, b.ascii, b.delim, good_idx=idx, **kw)
+    # and one list per query
+    gen = torch.Generator(device="cpu")
+    gen.manual_seed(len(lengths))
+    idx2 = torch.randint(1, n + 1, (len(enc), 257), generator=gen, dtype=torch.int32).cuda()
+    got_2 = batched.sw_scan_queries(buf, lens, tpt, b.ascii, b.delim, good_idx=idx2, **kw)
+    for i, e in enumerate(enc):
+        exp = sw.sw_scan(e, b.ascii, b.delim, g0=1, n_targets=n, **kw)
+        assert torch.equal(got[i, :n], exp), i
+        exp_i = sw.sw_scan(e, b.ascii, b.delim, good_idx=idx, **kw)
+        assert torch.equal(got_i[i, :idx.numel()], exp_i), i
+        exp_2 = sw.sw_scan(e, b.ascii, b.delim, good_idx=idx2[i], **kw)
+        assert torch.equal(got_2[i, :257], exp_2), i
+
+
+def test_length_outside_the_launch_width_is_not_scored():
+    from sseqs_b200 import batched, dbtools
+    _, db = _db()
+    b = db.batches[0]
+    enc, buf, lens = _pack([dbtools.random_query(100, 1), dbtools.random_query(100, 2)])
+    lens[1] = 130                      # ceil(130/32) = 5, the launch is tpt 4
+    out = batched.sw_scan_queries(buf, lens, 4, b.ascii, b.delim, affine=True, g0=1,
+                                  n_targets=500, skip=1, gap_a=11, gap_b=1)
+    assert bool((out[1, :500] == torch.iinfo(torch.int32).min).all())
+    assert bool((out[0, :500] >= 0).all())
+
+
+def _per_query_topk(db, enc, k):
+    from sseqs_b200 import select
+    sw = importlib.import_module("sseqs_b200.sw")
+    rows = []
+    for bi, b in enumerate(db.batches):
+        n = b.n_segments - 2
+        if n <= 0:
+            continue
+        s = sw.sw_scan(enc, b.ascii, b.delim, affine=True, g0=1, n_targets=n, skip=1,
+                       gap_a=11, gap_b=1)
+        kk = min(k, n)
+        p = select.topk_indices(s, kk).long()
+        for t, v in zip(p.cpu().numpy(), s[p].cpu().numpy()):
+            rows.append((-int(v), bi, int(t) + 1))
+    rows.sort()
+    return rows[:k]
+
+
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_search_queries_matches_per_query_topk(use_graphs):
+    from sseqs_b200 import batched, dbtools
+    _, db = _db()
+    rng = np.random.default_rng(11)
+    lengths = [int(x) for x in np.clip(np.round(np.exp(rng.normal(np.log(300), 0.7, 9))), 16,
+                                       2048)]
+    lengths += [lengths[0], lengths[0] + 1, lengths[0]]   # same width: groups of 2 replay
+    queries = [dbtools.random_query(L, 200 + i) for i, L in enumerate(lengths)]
+    got = batched.search_queries(queries, db, top_k=50, use_graphs=use_graphs, group=2)
+    sw = importlib.import_module("sseqs_b200.sw")
+    for i, q in enumerate(queries):
+        exp = _per_query_topk(db, sw.encode_query(q), 50)
+        h = got[i]
+        mine = list(zip((-h.scores.astype(np.int64)).tolist(), h.batch.tolist(),
+                        h.segment.tolist()))
+        assert mine == exp, i

@@ -60,3 +60,12 @@ def test_fails_loudly_without_library(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(ImportError):
         _lib.lib()
+
+
+def test_batched_buckets_group_by_stripe_width():
+    from sseqs_b200 import batched
+    lengths = [300, 31, 32, 33, 2048, 64, 289, 1]
+    b = batched.buckets(lengths)
+    assert b == {10: [6, 0], 1: [7, 1, 2], 2: [3, 5], 64: [4]}
+    for tpt, members in b.items():
+        assert all((lengths[i] + 31) // 32 == tpt for i in members)
