@@ -1,28 +1,44 @@
-// Gapless low-rank correlation prefilter (the quantity of sseqs/fft.cu:17-415
-// with sseqs/filter.cu:92-159).
+// Gapless low-rank correlation prefilter: the quantity of sseqs/fft.cu:17-415
+// with sseqs/filter.cu:92-159, computed directly instead of by FFT.
 //
-// For a query q, rank-k look-up tables A (query side) and B (database side)
-// and a segment t, with N a power of two and H = N/2:
+// For a query q (Lq residues), rank-k look-up tables A (query side) and B
+// (database side), a segment t (Lt <= N bytes) and N a power of two:
 //   a_r[i] = A_r[pos(q[Lq-1-i])] (i < Lq),   b_r[i] = B_r[pos(t[i])] (i < Lt),
 //   y      = sum_r a_r (*) b_r                (cyclic convolution of length N)
-//   score  = fp16( 0.5 * max_n y[2n] )        (even lags only)
+//   score  = fp16( 0.5 * max over even s of y[s] )
 // pos() maps ARNDCQEGHILKMFPSTWYV to 0..19, X - * to 20 and any other byte to
 // 21; B_r[21] is B_{r+1}[0] (the reference reads one entry past the row,
 // sseqs/fft.cu:91,124) and 0 for the last rank.
 //
-// B200 mapping: one warp per segment, fp32.  Real inputs of length N are
-// packed as z[n] = x[2n] + i x[2n+1] and transformed by a 32-lane radix-2
-// FFT of length H (H/32 complex values per lane; stages whose butterfly
-// partner lives in another lane exchange through __shfl_xor_sync).  The
-// forward transform is decimation-in-time on bit-reversed input (natural
-// order out), the rank products are summed in the frequency domain
-// (P = sum_r Q_r X_r), and a single decimation-in-frequency inverse follows
-// -- its output order does not matter because only the maximum is kept.
-// The query spectra Q_r are computed once per (query, N) by the same code.
-// Twiddles come from a shared table filled with sincospif.
+// Direct form.  With j = Lq-1-i the forward query position, the linear
+// correlation c[m] = sum_i a[i] b[m-i] is the sum of P(j, t[p]) along the
+// diagonal p - j = m - (Lq-1) of the Lq x Lt matrix, where
+//   P(j, c) = sum_r A_r[pos(q[j])] * B_r[c]
+// is a per-query profile; and the cyclic y folds c once: y[s] = c[s] +
+// c[s+N] (c has Lq+Lt-1 <= 2N entries), with y[s] = 0 for lags that no
+// diagonal reaches.  So every score is a set of fp32 diagonal sums: one add
+// per (query, target) cell, about Lq*Lt/2 useful ones per segment, instead of
+// k+1 transforms of length N (N is set by the longest segment of the batch).
+//
+// B200 mapping: one warp per segment, lane l holding C = ceil(Lq/32)
+// consecutive query columns (the query is left-padded to 32C columns with
+// zero profile entries), D(j) the running sum of the diagonal ending at
+// (row, j).  A row is D(j) <- D(j-1) + P(j, t[row]): a shift by one column
+// (one shuffle crosses the lane boundary) and C adds.  Reading the profile
+// is what bounds the kernel (shared-memory bandwidth: a profile entry per
+// cell), so it is stored as fp16 -- half the bytes -- and each add takes the
+// fp16 entry and the fp32 running sum in one instruction (add.f32.f16; the
+// sums stay fp32).  The profile sits in shared memory, 32C entries per class,
+// each lane's columns padded to an odd number of 16-byte units so the
+// 128-bit loads of a warp do not conflict.  The value leaving the last column at row s is c[s]; it enters
+// the maximum at once unless its partner c[s+N] exists, in which case it is
+// parked in a per-warp shared array until the segment's last row, when the
+// remaining diagonals (m >= Lt) are read off every column.
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <array>
+#include <utility>
 
 #include "common.cuh"
 
@@ -30,131 +46,12 @@ namespace sseqs {
 namespace {
 
 constexpr int kMaxRank = 20;
-constexpr int kPfWarps = 4;
+constexpr int kPfClasses = 22;
 
 __device__ __forceinline__ int pf_pos(uint8_t c) {
   const uint8_t k = ascii_class(c);
   if (k < kNumAA) return k;
   return (c == 'X' || c == '-' || c == '*') ? 20 : 21;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
-  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
-}
-__device__ __forceinline__ float2 shfl2(float2 v, int src) {
-  return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-}
-
-// tw[k] = exp(-2 pi i k / N), k < H
-template <int LOG_H>
-__device__ void fill_twiddles(float2* tw) {
-  constexpr int H = 1 << LOG_H;
-  for (int k = threadIdx.x; k < H; k += blockDim.x) {
-    float s, c;
-    sincospif(-(float)k / (float)H, &s, &c);   // -2k/N = -k/H
-    tw[k] = make_float2(c, s);
-  }
-}
-
-// Forward DIT of v (bit-reversed input, natural output); lane l holds
-// indices l*T .. l*T+T-1.
-template <int LOG_H>
-__device__ __forceinline__ void fft_dit(float2 (&v)[(1 << LOG_H) / 32 > 0 ? (1 << LOG_H) / 32 : 1],
-                                        const float2* tw, int lane) {
-  constexpr int H = 1 << LOG_H, T = H / 32, N = 2 * H;
-  const int base = lane * T;
-#pragma unroll
-  for (int s = 0; s < LOG_H; ++s) {
-    const int half = 1 << s;
-    const int step = N / (2 * half);        // W_m^j = tw[j * N/m]
-    if (half < T) {
-#pragma unroll
-      for (int i = 0; i < T; ++i) {
-        const int g = base + i;
-        if ((g & half) == 0) {
-          const float2 w = tw[(g & (half - 1)) * step];
-          const float2 a = v[i], t = cmul(v[i ^ half], w);
-          v[i] = cadd(a, t);
-          v[i ^ half] = csub(a, t);
-        }
-      }
-    } else {
-      const int ld = half / T;
-#pragma unroll
-      for (int i = 0; i < T; ++i) {
-        const int g = base + i;
-        const float2 a = v[i], b = shfl_xor2(a, ld);
-        const float2 w = tw[(g & (half - 1)) * step];
-        v[i] = ((g & half) == 0) ? cadd(a, cmul(b, w)) : csub(b, cmul(a, w));
-      }
-    }
-  }
-}
-
-// Inverse DIF (natural input, bit-reversed output), unnormalised.
-template <int LOG_H>
-__device__ __forceinline__ void ifft_dif(float2 (&v)[(1 << LOG_H) / 32 > 0 ? (1 << LOG_H) / 32 : 1],
-                                         const float2* tw, int lane) {
-  constexpr int H = 1 << LOG_H, T = H / 32, N = 2 * H;
-  const int base = lane * T;
-#pragma unroll
-  for (int s = LOG_H - 1; s >= 0; --s) {
-    const int half = 1 << s;
-    const int step = N / (2 * half);
-    if (half < T) {
-#pragma unroll
-      for (int i = 0; i < T; ++i) {
-        const int g = base + i;
-        if ((g & half) == 0) {
-          const float2 w = conj2(tw[(g & (half - 1)) * step]);
-          const float2 a = v[i], b = v[i ^ half];
-          v[i] = cadd(a, b);
-          v[i ^ half] = cmul(csub(a, b), w);
-        }
-      }
-    } else {
-      const int ld = half / T;
-#pragma unroll
-      for (int i = 0; i < T; ++i) {
-        const int g = base + i;
-        const float2 a = v[i], b = shfl_xor2(a, ld);
-        const float2 w = conj2(tw[(g & (half - 1)) * step]);
-        v[i] = ((g & half) == 0) ? cadd(a, b) : cmul(csub(b, a), w);
-      }
-    }
-  }
-}
-
-// After fft_dit of a packed real signal: X[k] for this lane's k (written to
-// X[]), and X[H] (returned; meaningful on lane 0).
-template <int LOG_H>
-__device__ __forceinline__ float unpack_real(float2 (&v)[(1 << LOG_H) / 32 > 0 ? (1 << LOG_H) / 32 : 1],
-                                             float2 (&X)[(1 << LOG_H) / 32 > 0 ? (1 << LOG_H) / 32 : 1],
-                                             const float2* tw, int lane) {
-  constexpr int H = 1 << LOG_H, T = H / 32;
-  float xh = 0.f;
-#pragma unroll
-  for (int j = 0; j < T; ++j) {
-    const int k = lane * T + j;
-    const int mj = (j == 0) ? 0 : T - j;
-    const int ml = (j == 0) ? ((32 - lane) & 31) : 31 - lane;
-    const float2 gm = shfl2(v[mj], ml);
-    if (k == 0) {
-      X[j] = make_float2(v[0].x + v[0].y, 0.f);
-      xh = v[0].x - v[0].y;
-    } else {
-      const float2 S = cadd(v[j], conj2(gm)), D = csub(v[j], conj2(gm));
-      const float2 WD = cmul(tw[k], D);
-      X[j] = make_float2(0.5f * (S.x + WD.y), 0.5f * (S.y - WD.x));
-    }
-  }
-  return xh;
 }
 
 struct PfArgs {
@@ -167,141 +64,164 @@ struct PfArgs {
   const uint8_t* qrev;      // query positions, reversed, already mapped (0..20)
   int Lq;
   int k;
-  float2* qspec;            // [k][H+1]
+  int N;                    // cyclic length
   __half* out;              // [n]
 };
 
-// One warp per rank: Q_r = DFT_N(a_r), k = 0..H.
-template <int LOG_H>
-__global__ void __launch_bounds__(32) query_spectrum_kernel(PfArgs a) {
-  constexpr int H = 1 << LOG_H, T = H / 32, N = 2 * H;
-  __shared__ float2 tw[H];
-  fill_twiddles<LOG_H>(tw);
-  __syncwarp();
-  const int r = blockIdx.x, lane = threadIdx.x;
-  if (r >= a.k) return;
-  float2 v[T], X[T];
-#pragma unroll
-  for (int j = 0; j < T; ++j) {
-    const int p = (int)(__brev((unsigned)(lane * T + j)) >> (32 - LOG_H));
-    const int i0 = 2 * p, i1 = 2 * p + 1;
-    const float x0 = (i0 < a.Lq && i0 < N) ? a.A[r * 21 + a.qrev[i0]] : 0.f;
-    const float x1 = (i1 < a.Lq && i1 < N) ? a.A[r * 21 + a.qrev[i1]] : 0.f;
-    v[j] = make_float2(x0, x1);
-  }
-  fft_dit<LOG_H>(v, tw, lane);
-  const float xh = unpack_real<LOG_H>(v, X, tw, lane);
-  float2* row = a.qspec + (int64_t)r * (H + 1);
-#pragma unroll
-  for (int j = 0; j < T; ++j) row[lane * T + j] = X[j];
-  if (lane == 0) row[H] = make_float2(xh, 0.f);
+template <int C>
+struct PfShape {
+  static constexpr int NV = (C + 7) / 8;                       // 128-bit loads per row
+  static constexpr int LW = ((NV % 2) ? NV : NV + 1) * 8;      // fp16 entries per lane (odd x 16 B)
+  static constexpr int ROW = 32 * LW;                          // entries per class
+  static constexpr int WARPS = C <= 32 ? 16 : 8;
+  static constexpr int PARK = 16 * C;                          // parked c[s] per warp (even s)
+  static constexpr size_t smem = sizeof(__half) * (size_t)kPfClasses * ROW +
+                                 sizeof(float) * (size_t)WARPS * PARK + 256;
+};
+
+// fp32 + fp16 -> fp32 in one instruction
+__device__ __forceinline__ float add_f32_f16(float acc, unsigned short h) {
+  float r;
+  asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(h), "f"(acc));
+  return r;
 }
 
-template <int LOG_H>
-__global__ void __launch_bounds__(32 * kPfWarps) prefilter_kernel(PfArgs a) {
-  constexpr int H = 1 << LOG_H, T = H / 32, N = 2 * H;
+template <int C>
+__global__ void __launch_bounds__(32 * PfShape<C>::WARPS) prefilter_kernel(PfArgs a) {
+  using S = PfShape<C>;
+  constexpr int J = 32 * C;
   extern __shared__ float4 smem_pf[];
-  float2* tw = reinterpret_cast<float2*>(smem_pf);                 // H
-  float2* Q = tw + H;                                             // k*(H+1)
-  float* Bt = reinterpret_cast<float*>(Q + a.k * (H + 1));        // k*23
-  uint8_t* cls_all = reinterpret_cast<uint8_t*>(Bt + a.k * 23);   // warps*N
-  fill_twiddles<LOG_H>(tw);
-  for (int i = threadIdx.x; i < a.k * (H + 1); i += blockDim.x) Q[i] = a.qspec[i];
-  for (int i = threadIdx.x; i < a.k * 23; i += blockDim.x) {
-    const int r = i / 23, c = i % 23;
-    float v = 0.f;
-    if (c < 21) v = a.B[r * 21 + c];
-    else if (c == 21) v = (r + 1 < a.k) ? a.B[(r + 1) * 21] : 0.f;
-    Bt[i] = v;                                                    // class 22: padding, 0
+  __half* prof = reinterpret_cast<__half*>(smem_pf);               // [22][ROW]
+  float* park_all = reinterpret_cast<float*>(prof + kPfClasses * S::ROW);   // [WARPS][PARK]
+  uint8_t* lut = reinterpret_cast<uint8_t*>(park_all + S::WARPS * S::PARK);
+
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = (uint8_t)pf_pos((uint8_t)i);
+  // profile: column j of lane l = j / C sits at l*LW + j % C; real query
+  // column jr = j - (J - Lq) (left padding), its residue q[jr] = qrev[Lq-1-jr]
+  const int pad = J - a.Lq;
+  for (int i = threadIdx.x; i < kPfClasses * S::ROW; i += blockDim.x) {
+    const int c = i / S::ROW, r = i - c * S::ROW;
+    const int l = r / S::LW, v = r - l * S::LW;
+    const int jr = l * C + v - pad;
+    float p = 0.f;
+    if (v < C && jr >= 0) {
+      const int qa = a.qrev[a.Lq - 1 - jr];
+      for (int rk = 0; rk < a.k; ++rk) {
+        const float bv = c < 21 ? a.B[rk * 21 + c] : (rk + 1 < a.k ? a.B[(rk + 1) * 21] : 0.f);
+        p = fmaf(a.A[rk * 21 + qa], bv, p);
+      }
+    }
+    prof[i] = __float2half_rn(p);
   }
   __syncthreads();
+
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  uint8_t* cls = cls_all + wib * N;
-  const int64_t nwarps = (int64_t)gridDim.x * kPfWarps;
-  for (int64_t s = (int64_t)blockIdx.x * kPfWarps + wib; s < a.n; s += nwarps) {
+  float* park = park_all + wib * S::PARK;
+  const uint4* myprof = reinterpret_cast<const uint4*>(prof + lane * S::LW);
+  const int64_t nwarps = (int64_t)gridDim.x * S::WARPS;
+  const int N = a.N, Lq = a.Lq;
+  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
+  const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
+  const int64_t aoff = (int64_t)(au & 3);
+
+  for (int64_t s = (int64_t)blockIdx.x * S::WARPS + wib; s < a.n; s += nwarps) {
     const int len = min((int)a.lengths[s], N);
-    const uint8_t* t = a.ascii + a.offsets[s];
-    for (int i = lane; i < N; i += 32) cls[i] = i < len ? (uint8_t)pf_pos(t[i]) : (uint8_t)22;
-    __syncwarp();
-    float2 P[T];
-    float ph = 0.f;
+    const int64_t base = a.offsets[s];
+    // lags s' <= nlim have both c[s'] and c[s'+N]
+    const int nlim = Lq + len - 2 - N;
+    float D[C];
 #pragma unroll
-    for (int j = 0; j < T; ++j) P[j] = make_float2(0.f, 0.f);
-    for (int r = 0; r < a.k; ++r) {
-      const float* br = Bt + r * 23;
-      float2 v[T];
+    for (int k = 0; k < C; ++k) D[k] = 0.f;
+    float best = -INFINITY;
+    for (int i0 = 0; i0 < len; i0 += 4) {
+      // four target bytes from the two aligned words that hold them (a word
+      // is read only when it holds a byte of the segment)
+      const int64_t ap = base + i0 + aoff;
+      const int64_t wi = ap >> 2;
+      const uint32_t w0 = __ldg(abase + wi);
+      const uint32_t w1 = ((wi + 1) << 2) < base + len + aoff ? __ldg(abase + wi + 1) : 0u;
+      const uint32_t raw = __funnelshift_r(w0, w1, (uint32_t)(ap & 3) * 8u);
+      const int rows = min(4, len - i0);
 #pragma unroll
-      for (int j = 0; j < T; ++j) {
-        const int p = (int)(__brev((unsigned)(lane * T + j)) >> (32 - LOG_H));
-        v[j] = make_float2(br[cls[2 * p]], br[cls[2 * p + 1]]);
-      }
-      fft_dit<LOG_H>(v, tw, lane);
-      // unpack X_r[k] (as unpack_real) and accumulate P += Q_r X_r at once;
-      // v is only read here, so the mate values stay valid
-      const float2* q = Q + r * (H + 1);
+      for (int r = 0; r < 4; ++r) {
+        if (r < rows) {
+          const int cls = lut[(raw >> (8 * r)) & 0xffu];
+          const uint4* pr = myprof + cls * (S::ROW / 8);
+          unsigned short P[S::NV * 8];
 #pragma unroll
-      for (int j = 0; j < T; ++j) {
-        const int k = lane * T + j;
-        const int mj = (j == 0) ? 0 : T - j;
-        const int ml = (j == 0) ? ((32 - lane) & 31) : 31 - lane;
-        const float2 gm = shfl2(v[mj], ml);
-        float2 X;
-        if (k == 0) {
-          X = make_float2(v[0].x + v[0].y, 0.f);
-          ph += q[H].x * (v[0].x - v[0].y);
-        } else {
-          const float2 S = cadd(v[j], conj2(gm)), D = csub(v[j], conj2(gm));
-          const float2 WD = cmul(tw[k], D);
-          X = make_float2(0.5f * (S.x + WD.y), 0.5f * (S.y - WD.x));
+          for (int v = 0; v < S::NV; ++v) {
+            const uint4 x = pr[v];
+            const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+              asm("mov.b32 {%0, %1}, %2;" : "=h"(P[8 * v + 2 * h]), "=h"(P[8 * v + 2 * h + 1])
+                  : "r"(w[h]));
+          }
+          float left = __shfl_up_sync(0xffffffffu, D[C - 1], 1);
+          if (lane == 0) left = 0.f;
+#pragma unroll
+          for (int k = C - 1; k > 0; --k) D[k] = add_f32_f16(D[k - 1], P[k]);
+          D[0] = add_f32_f16(left, P[0]);
+          const int row = i0 + r;
+          if (lane == 31 && (row & 1) == 0) {          // c[row] leaves the last column
+            if (row <= nlim) park[row >> 1] = D[C - 1];
+            else best = fmaxf(best, D[C - 1]);
+          }
         }
-        P[j] = cadd(P[j], cmul(q[k], X));
       }
     }
     __syncwarp();
-    // pack Z[k] = DFT_H(y_even + i y_odd) from P = DFT_N(y)
-    float2 Z[T];
+    // diagonals m = len + Lq - 2 - jr ending on the last row (jr <= Lq - 2)
+    if (len > 0) {
 #pragma unroll
-    for (int j = 0; j < T; ++j) {
-      const int k = lane * T + j;
-      const int mj = (j == 0) ? 0 : T - j;
-      const int ml = (j == 0) ? ((32 - lane) & 31) : 31 - lane;
-      const float2 pm = shfl2(P[mj], ml);
-      if (k == 0) {
-        Z[j] = make_float2(0.5f * (P[0].x + ph), 0.5f * (P[0].x - ph));
-      } else {
-        const float2 S = cadd(P[j], conj2(pm)), D = csub(P[j], conj2(pm));
-        const float2 WD = cmul(conj2(tw[k]), D);
-        Z[j] = make_float2(0.5f * (S.x - WD.y), 0.5f * (S.y + WD.x));
+      for (int k = 0; k < C; ++k) {
+        const int jr = lane * C + k - (J - Lq);
+        const int m = len + Lq - 2 - jr;
+        if (jr >= 0 && jr <= Lq - 2 && (m & 1) == 0) {
+          float v = D[k];
+          if (m >= N) v += park[(m - N) >> 1];
+          best = fmaxf(best, v);
+        }
       }
     }
-    ifft_dif<LOG_H>(Z, tw, lane);
-    float m = Z[0].x;
+    // even lags that no diagonal reaches have y = 0 (all of them when the
+    // query or the segment is empty)
+    if (len == 0 || Lq == 0 || Lq + len - 1 <= N - 2) best = fmaxf(best, 0.f);
 #pragma unroll
-    for (int j = 1; j < T; ++j) m = fmaxf(m, Z[j].x);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) a.out[s] = __float2half_rn(m * (0.5f / (float)H));
+    for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) a.out[s] = __float2half_rn(0.5f * best);
     __syncwarp();
   }
 }
 
-template <int LOG_H>
-int launch_pf(PfArgs a, cudaStream_t stream) {
-  constexpr int H = 1 << LOG_H, N = 2 * H;
-  { query_spectrum_kernel<LOG_H><<<a.k, 32, 0, stream>>>(a); count_launches(1); }
-  if (a.n == 0) return status_of(cudaGetLastError());
-  const size_t smem = sizeof(float2) * (H + (size_t)a.k * (H + 1)) + sizeof(float) * a.k * 23 +
-                      (size_t)kPfWarps * N;
-  if (cudaFuncSetAttribute(prefilter_kernel<LOG_H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+// ------------------------------------------------------------ dispatch
+using PfFn = void (*)(PfArgs);
+struct PfInfo {
+  PfFn fn;
+  size_t smem;
+  int threads;
+};
+
+template <int... I>
+std::array<PfInfo, sizeof...(I)> pf_table(std::integer_sequence<int, I...>) {
+  return {{PfInfo{prefilter_kernel<I + 1>, PfShape<I + 1>::smem, 32 * PfShape<I + 1>::WARPS}...}};
+}
+
+int launch_pf(const PfArgs& a, cudaStream_t stream) {
+  static const auto table = pf_table(std::make_integer_sequence<int, 64>{});
+  const int C = std::max(1, (a.Lq + 31) / 32);
+  const PfInfo& info = table[C - 1];
+  if (cudaFuncSetAttribute((const void*)info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)info.smem) != cudaSuccess)
     return SSEQS_ERR_CUDA;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, prefilter_kernel<LOG_H>, 32 * kPfWarps,
-                                                    smem) != cudaSuccess || nb < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)info.fn, info.threads,
+                                                    info.smem) != cudaSuccess || nb < 1)
     return SSEQS_ERR_CUDA;
-  const int64_t need = (a.n + kPfWarps - 1) / kPfWarps;
+  const int warps = info.threads / 32;
+  const int64_t need = (a.n + warps - 1) / warps;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * nb));
-  { prefilter_kernel<LOG_H><<<grid, 32 * kPfWarps, smem, stream>>>(a); count_launches(1); }
+  { info.fn<<<grid, info.threads, info.smem, stream>>>(a); count_launches(1); }
   return status_of(cudaGetLastError());
 }
 
@@ -312,7 +232,7 @@ using namespace sseqs;
 
 extern "C" size_t sseqs_prefilter_workspace_bytes(int n, int k) {
   if (n < 2 || k < 1) return 0;
-  return sizeof(float2) * (size_t)k * (size_t)(n / 2 + 1) + 256;
+  return 256;
 }
 
 extern "C" int sseqs_prefilter(const uint8_t* ascii, const int64_t* offsets, const int32_t* lengths,
@@ -326,15 +246,8 @@ extern "C" int sseqs_prefilter(const uint8_t* ascii, const int64_t* offsets, con
   if (!lut_a || !lut_b || (query_len > 0 && !query_pos_reversed)) return SSEQS_ERR_ARG;
   if (n_segments > 0 && (!ascii || !offsets || !lengths || !out_scores)) return SSEQS_ERR_ARG;
   if (!workspace || ws_bytes < sseqs_prefilter_workspace_bytes(n, k)) return SSEQS_ERR_WORKSPACE;
-  PfArgs a{ascii, offsets, lengths, n_segments, lut_a, lut_b, query_pos_reversed, query_len, k,
-           reinterpret_cast<float2*>(workspace), reinterpret_cast<__half*>(out_scores)};
-  switch (n) {
-    case 64: return launch_pf<5>(a, stream);
-    case 128: return launch_pf<6>(a, stream);
-    case 256: return launch_pf<7>(a, stream);
-    case 512: return launch_pf<8>(a, stream);
-    case 1024: return launch_pf<9>(a, stream);
-    case 2048: return launch_pf<10>(a, stream);
-  }
-  return SSEQS_ERR_UNSUPPORTED;
+  if (n_segments == 0) return SSEQS_OK;
+  PfArgs a{ascii, offsets, lengths, n_segments, lut_a, lut_b, query_pos_reversed, query_len, k, n,
+           reinterpret_cast<__half*>(out_scores)};
+  return launch_pf(a, stream);
 }
