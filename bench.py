@@ -257,6 +257,40 @@ def batched_leg(db, n_queries, seed=3):
             "cells": cells, "identical_hits": bool(same)}
 
 
+def serving_leg(db, n_requests, rate, seed=4):
+    """Request loop over the resident database (``serve.SearchServer`` with
+    the GPU executor): Poisson arrivals at ``rate`` queries/s, query lengths
+    U(50, 1000), exact affine scoring of every segment and top-4096 per
+    request, continuous batching at database-batch granularity.  Reports
+    completed queries/s and latency percentiles (submission to result)."""
+    from sseqs_b200 import dbtools, serve
+    rng = np.random.default_rng(seed)
+    queries = [dbtools.random_query(int(L), 9000 + i)
+               for i, L in enumerate(rng.integers(50, 1001, n_requests))]
+    ex = serve.GpuExecutor(db, top_k=TOP_K)
+    srv = serve.SearchServer(ex, top_k=TOP_K, max_slots=64)
+    # warm-up outside the measurement (autotune of the widths, first launches)
+    from sseqs_b200 import tune
+    tune.autotune([len(q) for q in queries], db.batches[0])
+    srv.submit(queries[0])
+    while srv.step():
+        pass
+    srv.completed.clear()
+    srv.start()
+    try:
+        offs = serve.poisson_arrivals(n_requests, rate, seed=seed)
+        reqs = serve.replay(srv, queries, offs)
+    finally:
+        srv.stop()
+    span = max(r.t_done for r in reqs) - min(r.t_submit for r in reqs)
+    st = serve.stats(reqs, span)
+    return {"requests": n_requests, "arrival_rate_qps": rate,
+            "queries_per_s": round(st.queries_per_s, 3), "p50_ms": round(st.p50_ms, 1),
+            "p99_ms": round(st.p99_ms, 1), "mean_ms": round(st.mean_ms, 1),
+            "engine_steps": srv.steps, "pipeline": "exact affine SW of every segment, top-4096",
+            "lengths": "U(50, 1000), seed %d" % seed}
+
+
 def measured_peak(name):
     """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
     int pipes), in int16x2 lane-instructions per second."""
@@ -459,6 +493,8 @@ def bench_b200(args):
         out["prefiltered"] = prefiltered_leg(M, db, timed[:args.prefilter_steps], exact_rows)
     if world == 1 and args.batched_queries > 0:
         out["batched"] = batched_leg(db, args.batched_queries)
+    if world == 1 and args.serve_requests > 0:
+        out["serving"] = serving_leg(db, args.serve_requests, args.serve_rate)
     if world == 1 and not args.no_cpu_baseline:
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
@@ -523,6 +559,10 @@ def main():
                     help="queries of the prefiltered (FFT) leg; 0 skips it")
     ap.add_argument("--batched-queries", type=int, default=16,
                     help="queries of the batched uneven-length leg; 0 skips it")
+    ap.add_argument("--serve-requests", type=int, default=24,
+                    help="requests of the serving leg; 0 skips it")
+    ap.add_argument("--serve-rate", type=float, default=1.5,
+                    help="Poisson arrival rate (queries/s) of the serving leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
