@@ -240,6 +240,85 @@ int sseqs_sw_set_variant(int affine, int tpt, int wide);
 /* int16x2 words per lane of a variant (for reports); -1 if out of range. */
 int sseqs_sw_variant_words(int affine, int tpt, int wide);
 
+/* ------------------------------------------------- learned prefilter
+ * No reference counterpart: a trained embedding stands in for the FFT
+ * prefilter stage (sseqs/msa.py:110-307) as a way to choose candidates for
+ * exact SW.  Layout of a set of sequences: row-major bf16 [P x C]
+ * activations, each sequence followed by >= 2 zero rows and preceded by 2
+ * (row0 of the first sequence >= 2), buffers with 2 addressable zero rows
+ * before row 0 and after row P-1.  Classes: 0..19 ARNDCQEGHILKMFPSTWYV,
+ * 20 other residues, 255 padding.  bf16 data are __nv_bfloat16. */
+
+/* C = op(A) . op(B)^T over K (K % 32 == 0): A is [M x K] (a_t = 0, row
+ * stride lda) or stored [K x M] (a_t = 1); B is [N x K] (b_t = 0) or
+ * stored [K x N] (b_t = 1); supported (a_t, b_t): (0, 0) with every
+ * epilogue, (1, 1) with epilogue 0.  Epilogue 0: C fp32; 1: C bf16;
+ * 2: C2 = acc + bias (bf16 pre-activation), C = GELU(C2) (bf16, tanh form);
+ * 3: C = acc * GELU'(aux) (bf16, aux bf16 with C's stride).  row_mask
+ * (nullable, uint8 per row of C): rows with 0 are written as 0 (epilogues
+ * 1-3).  A, B 16-byte aligned, lda, ldb multiples of 8; a_t needs M % 8 ==
+ * 0, b_t N % 8 == 0.  Tensor cores (mma.sync bf16, fp32 accumulation). */
+int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_t K,
+                    const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
+                    int64_t ldc, void* C2, const float* bias, const void* aux,
+                    const uint8_t* row_mask, cudaStream_t stream);
+
+/* cls[row0[s] + i] = class of ascii[off[s] + i] for i < len[s] (other rows
+ * untouched). */
+int sseqs_embed_layout(const uint8_t* ascii, const int64_t* off, const int32_t* len,
+                       const int64_t* row0, int n_seqs, uint8_t* cls, cudaStream_t stream);
+/* X[p][c] = E[cls[p]][c] (bf16, E [21][D]); 0 for padding rows. */
+int sseqs_embed_lookup(const uint8_t* cls, int64_t P, const void* E, int D, void* X,
+                       cudaStream_t stream);
+/* dE[cls[p]][c] += dX[p][c] (fp32 dE, bf16 dX). */
+int sseqs_embed_grad(const uint8_t* cls, int64_t P, const void* dX, int D, float* dE,
+                     cudaStream_t stream);
+/* Per sequence s: pooled = mean of rows start[s] .. + len[s] of Y [P x D]
+ * (bf16), emb = pooled / |pooled|, inv_norm = 1 / |pooled| (fp32). */
+int sseqs_pool_normalize(const void* Y, int D, const int64_t* start, const int32_t* len,
+                         int n_seqs, float* pooled, float* emb, float* inv_norm,
+                         cudaStream_t stream);
+/* For B pairs: pred = <emb[ia], emb[ib]>, *loss += (pred - y)^2 / B, and
+ * (dE non-null) dE[ia] += 2 (pred - y) / B * emb[ib], dE[ib] likewise;
+ * pred (nullable) receives the dot products. */
+int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const int32_t* ib,
+                    const float* y, int64_t B, float* dE, float* loss, float* pred,
+                    cudaStream_t stream);
+/* Gradient of pool_normalize back to the last layer's pre-activation Z:
+ * dZ[row] = (dE - emb <emb, dE>) * inv_norm / len * GELU'(Z[row]) for the
+ * rows of every sequence (other rows untouched). */
+int sseqs_pool_backward(const float* emb, const float* dE, const float* inv_norm,
+                        const int64_t* start, const int32_t* len, int n_seqs, int D,
+                        const void* Z, void* dZ, cudaStream_t stream);
+/* db[c] += sum over the P rows of dZ[p][c]. */
+int sseqs_bias_grad(const void* dZ, int64_t P, int D, float* db, cudaStream_t stream);
+/* Adam step of a conv weight W[Cout][5][Cin] (fp32 w, m, v) from dWT
+ * [5*Cin][Cout] (the weight-grad GEMM's output); writes bf16 Wb[co][t][ci]
+ * and Wf[ci][4-t][co]. */
+int sseqs_adam_conv(float* w, float* m, float* v, const float* dWT, int Cout, int Cin, float lr,
+                    float b1, float b2, float eps, int step, void* Wb, void* Wf,
+                    cudaStream_t stream);
+/* Adam step of n flat parameters; wb (nullable) receives a bf16 copy. */
+int sseqs_adam_flat(float* w, float* m, float* v, const float* g, int64_t n, float lr, float b1,
+                    float b2, float eps, int step, void* wb, cudaStream_t stream);
+/* out[i] = e4m3 code of scale * x[i] (saturating). */
+int sseqs_quantize_e4m3(const float* x, int64_t n, float scale, uint8_t* out,
+                        cudaStream_t stream);
+/* Candidate selection by FP8 GEMM (mma.sync e4m3, fp32 accumulation): for
+ * every query q (codes Q [nq][256]) and database row r (codes DB [n][256])
+ * with <Q[q], DB[r]> >= tau[q], appends r (and the dot product) to q's list:
+ * slot = count[q]++ (count zeroed by the caller), kept when slot < cap, at
+ * cand[q*cap + slot] / cand_score[q*cap + slot].  Q, DB 16-byte aligned. */
+int sseqs_score_select(const uint8_t* Q, int nq, const uint8_t* DB, int64_t n, const float* tau,
+                       int32_t* count, int64_t* cand, float* cand_score, int cap,
+                       cudaStream_t stream);
+/* Dense dot products out[q][r] = <Q[q], DB[r]> (fp32, [nq][n]). */
+int sseqs_score_dense(const uint8_t* Q, int nq, const uint8_t* DB, int64_t n, float* out,
+                      cudaStream_t stream);
+/* out[r] = k-th largest of row r of x [rows][n] (n <= 8192). */
+int sseqs_kth_largest_rows(const float* x, int rows, int n, int k, float* out,
+                           cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,869 @@
+// Kernels of the learned prefilter: a 1D-conv sequence embedder (forward and
+// backward in BF16 on the tensor cores, fp32 accumulation), its optimiser,
+// and the FP8 database scoring GEMM with fused candidate selection.
+//
+// Activations of a set of sequences live in one row-major [P x C] bf16
+// matrix: the sequences one after another, each followed by at least two
+// zero rows, with two zero rows before the first.  A width-5 convolution
+// then needs no im2col buffer: the 5 input rows p-2 .. p+2 of output row p
+// are contiguous, so im2col(X) is the [P x 5C] matrix whose row p starts at
+// X + (p-2)*C (row stride C, rows overlapping).  Every layer is a GEMM on
+// such views:
+//   forward      Z   = im2col(Y_prev) . W^T + b      W  [Cout][5][Cin]
+//   data grad    dY  = im2col(dZ) . Wf^T             Wf [Cin][5][Cout], Wf[ci][t][co] = W[co][4-t][ci]
+//   weight grad  dW^T = im2col(Y_prev)^T . dZ         (K = positions)
+// with the epilogues fused: bias + GELU (keeping Z for the backward pass),
+// GELU' times the incoming gradient, and a row mask that keeps padding rows
+// at zero (so the next layer's window reads zeros there, and no gradient
+// flows from them).
+//
+// The GEMM is a 128x128x32 tile per CTA, 8 warps of 64x32, mma.sync
+// m16n8k16 bf16 -> fp32 fed by ldmatrix (.trans for operands stored with M
+// or N contiguous), three cp.async stages.  The database scoring GEMM is
+// FP8 e4m3 (mma.sync m16n8k32): each CTA keeps 128 queries' embeddings in
+// shared memory and streams 128-row database tiles, and its epilogue appends
+// every (query, row) whose score reaches the query's threshold to that
+// query's candidate list -- the [queries x database] score matrix is never
+// written.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace sseqs {
+namespace emb {
+
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, GEMM_THREADS = 256;
+constexpr int LDK = BK + 8;        // [row][k] tile row, elements (80 B: ldmatrix conflict-free)
+constexpr int LDR = BM + 8;        // [k][row] tile row, elements (272 B)
+
+enum Epi : int {
+  EPI_F32 = 0,          // C (fp32) = acc
+  EPI_BF16 = 1,         // C (bf16) = acc  (masked rows -> 0)
+  EPI_BIAS_GELU = 2,    // Z = acc + bias (bf16, C2), C = gelu(Z) (bf16); masked rows -> 0
+  EPI_GELU_GRAD = 3,    // C (bf16) = acc * gelu'(aux);  masked rows -> 0
+};
+
+__device__ __forceinline__ float gelu_f(float z) {
+  const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
+  return 0.5f * z * (1.f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
+  const float t = tanhf(u);
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * 0.7978845608f * (1.f + 0.134145f * z * z);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool pred) {
+  const int n = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+struct GemmArgs {
+  int64_t M, N, K;
+  const __nv_bfloat16* A;
+  int64_t lda;
+  const __nv_bfloat16* B;
+  int64_t ldb;
+  void* C;
+  int64_t ldc;
+  __nv_bfloat16* C2;          // EPI_BIAS_GELU: pre-activation
+  const float* bias;
+  const __nv_bfloat16* aux;   // EPI_GELU_GRAD: pre-activation
+  const uint8_t* row_mask;    // nullable: 0 = padding row
+};
+
+// A_T: A stored [K][M] (element (m,k) at A[k*lda + m]) instead of [M][K].
+// B_T: B stored [K][N] instead of [N][K].
+template <bool A_T, bool B_T, int EPI>
+__global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
+  constexpr int A_TILE = A_T ? BK * LDR : BM * LDK;
+  constexpr int B_TILE = B_T ? BK * LDR : BN * LDK;
+  extern __shared__ __align__(16) unsigned char gsm[];
+  __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(gsm);
+  __nv_bfloat16* sB = sA + STAGES * A_TILE;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;          // 2 x 4 warps of 64 x 32
+  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+  const int64_t ktiles = g.K / BK;
+
+  auto load_tile = [&](int stage, int64_t kt) {
+    const int64_t k0 = kt * BK;
+    __nv_bfloat16* a = sA + stage * A_TILE;
+    __nv_bfloat16* b = sB + stage * B_TILE;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int c = tid + it * GEMM_THREADS;        // 512 16-byte chunks per operand
+      if (!A_T) {
+        const int r = c >> 2, kc = (c & 3) * 8;
+        const int64_t m = m0 + r;
+        const bool ok = m < g.M;
+        cp_async16(a + r * LDK + kc, g.A + (ok ? m : 0) * g.lda + k0 + kc, ok);
+      } else {
+        const int r = c >> 4, mc = (c & 15) * 8;
+        const int64_t m = m0 + mc;
+        const bool ok = m < g.M;
+        cp_async16(a + r * LDR + mc, g.A + (k0 + r) * g.lda + (ok ? m : 0), ok);
+      }
+      if (!B_T) {
+        const int r = c >> 2, kc = (c & 3) * 8;
+        const int64_t n = n0 + r;
+        const bool ok = n < g.N;
+        cp_async16(b + r * LDK + kc, g.B + (ok ? n : 0) * g.ldb + k0 + kc, ok);
+      } else {
+        const int r = c >> 4, nc = (c & 15) * 8;
+        const int64_t n = n0 + nc;
+        const bool ok = n < g.N;
+        cp_async16(b + r * LDR + nc, g.B + (k0 + r) * g.ldb + (ok ? n : 0), ok);
+      }
+    }
+  };
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) load_tile(s, s);
+    cp_commit();
+  }
+
+  for (int64_t kt = 0; kt < ktiles; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int64_t nk = kt + STAGES - 1;
+      if (nk < ktiles) load_tile((int)(nk % STAGES), nk);
+      cp_commit();
+    }
+    const __nv_bfloat16* a = sA + (kt % STAGES) * A_TILE;
+    const __nv_bfloat16* b = sB + (kt % STAGES) * B_TILE;
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 16) {
+      uint32_t af[4][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int mr = wm * 64 + i * 16;
+        if (!A_T) {
+          ldsm_x4(af[i], a + (mr + (lane & 15)) * LDK + ks + (lane >> 4) * 8);
+        } else {
+          const int j = lane >> 3, r = lane & 7;   // matrix j: m-half j&1, k-half j>>1
+          ldsm_x4_t(af[i], a + (ks + (j >> 1) * 8 + r) * LDR + mr + (j & 1) * 8);
+        }
+      }
+#pragma unroll
+      for (int jp = 0; jp < 2; ++jp) {
+        const int nr = wn * 32 + jp * 16;
+        uint32_t t[4];
+        const int j = lane >> 3, r = lane & 7;     // matrix j: n-half j>>1, k-half j&1
+        if (!B_T) ldsm_x4(t, b + (nr + (j >> 1) * 8 + r) * LDK + ks + (j & 1) * 8);
+        else ldsm_x4_t(t, b + (ks + (j & 1) * 8 + r) * LDR + nr + (j >> 1) * 8);
+        bf[2 * jp][0] = t[0];
+        bf[2 * jp][1] = t[1];
+        bf[2 * jp + 1][0] = t[2];
+        bf[2 * jp + 1][1] = t[3];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bf[j][0], bf[j][1]);
+    }
+  }
+  cp_wait<0>();
+
+  // epilogue
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t m = m0 + wm * 64 + i * 16 + (lane >> 2) + h * 8;
+      if (m >= g.M) continue;
+      const bool keep = g.row_mask ? g.row_mask[m] != 0 : true;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t n = n0 + wn * 32 + j * 8 + (lane & 3) * 2;
+        if (n >= g.N) continue;
+        const bool two = n + 1 < g.N;
+        float v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+        if (EPI == EPI_F32) {
+          float* c = reinterpret_cast<float*>(g.C) + m * g.ldc + n;
+          c[0] = v0;
+          if (two) c[1] = v1;
+        } else if (EPI == EPI_BF16) {
+          if (!keep) v0 = v1 = 0.f;
+          __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
+          c[0] = __float2bfloat16_rn(v0);
+          if (two) c[1] = __float2bfloat16_rn(v1);
+        } else if (EPI == EPI_BIAS_GELU) {
+          const float z0 = v0 + g.bias[n], z1 = two ? v1 + g.bias[n + 1] : 0.f;
+          __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
+          __nv_bfloat16* z = g.C2 + m * g.ldc + n;
+          const __nv_bfloat16 zb0 = __float2bfloat16_rn(keep ? z0 : 0.f);
+          const __nv_bfloat16 zb1 = __float2bfloat16_rn(keep ? z1 : 0.f);
+          z[0] = zb0;
+          c[0] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb0)) : 0.f);
+          if (two) {
+            z[1] = zb1;
+            c[1] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb1)) : 0.f);
+          }
+        } else {   // EPI_GELU_GRAD
+          const __nv_bfloat16* ax = g.aux + m * g.ldc + n;
+          __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
+          c[0] = __float2bfloat16_rn(keep ? v0 * gelu_grad(__bfloat162float(ax[0])) : 0.f);
+          if (two) c[1] = __float2bfloat16_rn(keep ? v1 * gelu_grad(__bfloat162float(ax[1])) : 0.f);
+        }
+      }
+    }
+  }
+}
+
+template <bool A_T, bool B_T, int EPI>
+int launch_gemm(const GemmArgs& g, cudaStream_t stream) {
+  constexpr int A_TILE = A_T ? BK * LDR : BM * LDK;
+  constexpr int B_TILE = B_T ? BK * LDR : BN * LDK;
+  constexpr size_t smem = sizeof(__nv_bfloat16) * STAGES * (A_TILE + B_TILE);
+  auto fn = gemm_kernel<A_T, B_T, EPI>;
+  if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const dim3 grid((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM));
+  if (grid.y > 65535u) return SSEQS_ERR_UNSUPPORTED;
+  { fn<<<grid, GEMM_THREADS, smem, stream>>>(g); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+// ------------------------------------------------------------ elementwise
+// X0[p][c] = E[cls[p]][c] for real rows (cls < 21), 0 for padding (cls 255).
+__global__ void embed_lookup_kernel(const uint8_t* cls, int64_t P, const __nv_bfloat16* E, int D,
+                                    __nv_bfloat16* X) {
+  const int64_t total = P * D;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / D;
+    const int c = (int)(i - p * D), k = cls[p];
+    X[i] = k < 21 ? E[k * D + c] : __float2bfloat16_rn(0.f);
+  }
+}
+
+// dE[cls[p]][c] += dX[p][c]
+__global__ void embed_grad_kernel(const uint8_t* cls, int64_t P, const __nv_bfloat16* dX, int D,
+                                  float* dE) {
+  const int64_t total = P * D;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / D;
+    const int c = (int)(i - p * D), k = cls[p];
+    if (k < 21) atomicAdd(dE + k * D + c, __bfloat162float(dX[i]));
+  }
+}
+
+// One block of D = blockDim.x threads per sequence: pooled = mean of its
+// rows, emb = pooled / |pooled|.
+__global__ void pool_normalize_kernel(const __nv_bfloat16* Y, const int64_t* start,
+                                      const int32_t* len, float* pooled, float* emb,
+                                      float* inv_norm) {
+  const int s = blockIdx.x, c = threadIdx.x, D = blockDim.x;
+  const int n = len[s];
+  const __nv_bfloat16* y = Y + start[s] * D + c;
+  float acc = 0.f;
+  for (int p = 0; p < n; ++p) acc += __bfloat162float(y[(int64_t)p * D]);
+  const float mean = n > 0 ? acc / (float)n : 0.f;
+  __shared__ float red[32];
+  float sq = mean * mean;
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+  if ((c & 31) == 0) red[c >> 5] = sq;
+  __syncthreads();
+  if (c < 32) {
+    float v = c < (D >> 5) ? red[c] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (c == 0) red[0] = v;
+  }
+  __syncthreads();
+  const float inv = rsqrtf(fmaxf(red[0], 1e-24f));
+  pooled[(int64_t)s * D + c] = mean;
+  emb[(int64_t)s * D + c] = mean * inv;
+  if (c == 0) inv_norm[s] = inv;
+}
+
+// One warp per pair: pred = <e_a, e_b>; loss += (pred - y)^2 / B;
+// dE_a += 2 (pred - y) / B * e_b, dE_b likewise.
+__global__ void pair_loss_kernel(const float* emb, int D, const int32_t* ia, const int32_t* ib,
+                                 const float* y, int64_t B, float* dE, float* loss,
+                                 float* pred_out) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= B) return;
+  const float* ea = emb + (int64_t)ia[w] * D;
+  const float* eb = emb + (int64_t)ib[w] * D;
+  float d = 0.f;
+  for (int c = lane; c < D; c += 32) d += ea[c] * eb[c];
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+  const float r = d - y[w];
+  const float g = 2.f * r / (float)B;
+  if (lane == 0) {
+    atomicAdd(loss, r * r / (float)B);
+    if (pred_out) pred_out[w] = d;
+  }
+  if (dE) {
+    float* ga = dE + (int64_t)ia[w] * D;
+    float* gb = dE + (int64_t)ib[w] * D;
+    for (int c = lane; c < D; c += 32) {
+      atomicAdd(ga + c, g * eb[c]);
+      atomicAdd(gb + c, g * ea[c]);
+    }
+  }
+}
+
+// Gradient of the pooled, normalised embedding back to the last layer's
+// pre-activation: dpooled = (dE - e <e, dE>) * inv_norm; each real row of
+// sequence s gets dpooled / len, times gelu'(Z).
+__global__ void pool_backward_kernel(const float* emb, const float* dE, const float* inv_norm,
+                                     const int64_t* start, const int32_t* len,
+                                     const __nv_bfloat16* Z, __nv_bfloat16* dZ) {
+  const int s = blockIdx.x, c = threadIdx.x, D = blockDim.x;
+  const float e = emb[(int64_t)s * D + c], g = dE[(int64_t)s * D + c];
+  __shared__ float red[32];
+  float v = e * g;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((c & 31) == 0) red[c >> 5] = v;
+  __syncthreads();
+  if (c < 32) {
+    float t = c < (D >> 5) ? red[c] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (c == 0) red[0] = t;
+  }
+  __syncthreads();
+  const int n = len[s];
+  const float dp = (g - e * red[0]) * inv_norm[s] / (float)max(n, 1);
+  const int64_t base = start[s] * D + c;
+  for (int p = 0; p < n; ++p) {
+    const int64_t i = base + (int64_t)p * D;
+    dZ[i] = __float2bfloat16_rn(dp * gelu_grad(__bfloat162float(Z[i])));
+  }
+}
+
+// db[c] += sum over rows of dZ[p][c] (block: 256 columns x a row range)
+__global__ void bias_grad_kernel(const __nv_bfloat16* dZ, int64_t P, int D, float* db) {
+  const int c = threadIdx.x + blockIdx.y * blockDim.x;
+  if (c >= D) return;
+  const int64_t rows = (P + gridDim.x - 1) / gridDim.x;
+  const int64_t p0 = (int64_t)blockIdx.x * rows, p1 = min(P, p0 + rows);
+  float acc = 0.f;
+  for (int64_t p = p0; p < p1; ++p) acc += __bfloat162float(dZ[p * D + c]);
+  atomicAdd(db + c, acc);
+}
+
+struct AdamArgs {
+  float lr, b1, b2, eps, c1, c2;   // c1 = 1 - b1^t, c2 = 1 - b2^t
+};
+__device__ __forceinline__ float adam_step(float& w, float& m, float& v, float g,
+                                           const AdamArgs& o) {
+  m = o.b1 * m + (1.f - o.b1) * g;
+  v = o.b2 * v + (1.f - o.b2) * g * g;
+  w -= o.lr * (m / o.c1) / (sqrtf(v / o.c2) + o.eps);
+  return w;
+}
+
+// Conv weight W[co][t][ci] (fp32 master + moments) from its gradient in the
+// weight-grad GEMM's layout dWT[(t*Cin + ci)][co]; writes the bf16 copies
+// W[co][t][ci] and Wf[ci][4-t][co].
+__global__ void adam_conv_kernel(float* w, float* m, float* v, const float* dWT, int Cout,
+                                 int Cin, AdamArgs o, __nv_bfloat16* Wb, __nv_bfloat16* Wf) {
+  const int64_t total = (int64_t)Cout * 5 * Cin;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int co = (int)(i / (5 * Cin));
+    const int r = (int)(i - (int64_t)co * 5 * Cin);
+    const int t = r / Cin, ci = r - t * Cin;
+    const float g = dWT[(int64_t)(t * Cin + ci) * Cout + co];
+    const float nw = adam_step(w[i], m[i], v[i], g, o);
+    const __nv_bfloat16 b = __float2bfloat16_rn(nw);
+    Wb[i] = b;
+    Wf[((int64_t)ci * 5 + (4 - t)) * Cout + co] = b;
+  }
+}
+
+// Flat parameters (bias, residue embedding); optional bf16 copy.
+__global__ void adam_flat_kernel(float* w, float* m, float* v, const float* g, int64_t n,
+                                 AdamArgs o, __nv_bfloat16* wb) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float nw = adam_step(w[i], m[i], v[i], g[i], o);
+    if (wb) wb[i] = __float2bfloat16_rn(nw);
+  }
+}
+
+// e4m3 codes of scale * x
+__global__ void quantize_e4m3_kernel(const float* x, int64_t n, float scale, uint8_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint8_t)__nv_cvt_float_to_fp8(scale * x[i], __NV_SATFINITE, __NV_E4M3);
+}
+
+// ------------------------------------------------------ FP8 score + select
+constexpr int SK = 256;            // embedding width (bytes per e4m3 row)
+constexpr int SLD = SK + 16;       // smem row stride (272 B: ldmatrix conflict-free)
+
+__device__ __forceinline__ void mma_e4m3(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.f32.e4m3.e4m3.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+struct SelArgs {
+  const uint8_t* Q;        // [nq][256] e4m3
+  int nq;
+  const uint8_t* DB;       // [n][256] e4m3
+  int64_t n;
+  const float* tau;        // [nq] threshold on the raw dot product of the codes
+  int32_t* count;          // [nq]
+  int64_t* cand;           // [nq][cap] database rows
+  float* cand_score;       // [nq][cap]
+  int cap;
+};
+
+// CTA: 128 queries (blockIdx.y) x database tiles of 128 rows (blockIdx.x,
+// gridDim.x apart).  Two database stages in flight.
+__global__ void __launch_bounds__(GEMM_THREADS) score_select_kernel(SelArgs a) {
+  extern __shared__ __align__(16) unsigned char ssm[];
+  uint8_t* sQ = ssm;                         // [128][SLD]
+  uint8_t* sD = ssm + 128 * SLD;             // [2][128][SLD]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int q0 = blockIdx.y * 128;
+  // query tile (rows past nq are zero)
+  for (int c = tid; c < 128 * (SK / 16); c += GEMM_THREADS) {
+    const int r = c / (SK / 16), kc = (c % (SK / 16)) * 16;
+    const bool ok = q0 + r < a.nq;
+    cp_async16(sQ + r * SLD + kc, a.Q + (int64_t)(ok ? q0 + r : 0) * SK + kc, ok);
+  }
+  cp_commit();
+  const int64_t ntiles = (a.n + 127) / 128;
+  auto load_db = [&](int stage, int64_t tile) {
+    uint8_t* d = sD + stage * 128 * SLD;
+    for (int c = tid; c < 128 * (SK / 16); c += GEMM_THREADS) {
+      const int r = c / (SK / 16), kc = (c % (SK / 16)) * 16;
+      const int64_t row = tile * 128 + r;
+      const bool ok = row < a.n;
+      cp_async16(d + r * SLD + kc, a.DB + (ok ? row : 0) * SK + kc, ok);
+    }
+  };
+  int64_t tile = blockIdx.x;
+  if (tile < ntiles) load_db(0, tile);
+  cp_commit();
+  float tau[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = q0 + wm * 64 + i * 16 + (lane >> 2) + h * 8;
+      tau[i][h] = q < a.nq ? a.tau[q] : INFINITY;
+    }
+  int stage = 0;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int64_t next = tile + gridDim.x;
+    if (next < ntiles) load_db(stage ^ 1, next);
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();
+    const uint8_t* d = sD + stage * 128 * SLD;
+    float acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < SK; ks += 32) {
+      uint32_t af[4][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        ldsm_x4(af[i], sQ + (wm * 64 + i * 16 + (lane & 15)) * SLD + ks + (lane >> 4) * 16);
+#pragma unroll
+      for (int jp = 0; jp < 2; ++jp) {
+        uint32_t t[4];
+        const int j = lane >> 3, r = lane & 7;
+        ldsm_x4(t, d + (wn * 32 + jp * 16 + (j >> 1) * 8 + r) * SLD + ks + (j & 1) * 16);
+        bf[2 * jp][0] = t[0];
+        bf[2 * jp][1] = t[1];
+        bf[2 * jp + 1][0] = t[2];
+        bf[2 * jp + 1][1] = t[3];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_e4m3(acc[i][j], af[i], bf[j][0], bf[j][1]);
+    }
+    // epilogue: append every score that reaches its query's threshold
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = q0 + wm * 64 + i * 16 + (lane >> 2) + h * 8;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const float v = acc[i][j][2 * h + e];
+            const int64_t row = tile * 128 + wn * 32 + j * 8 + (lane & 3) * 2 + e;
+            if (v >= tau[i][h] && row < a.n) {
+              const int slot = atomicAdd(a.count + q, 1);
+              if (slot < a.cap) {
+                a.cand[(int64_t)q * a.cap + slot] = row;
+                a.cand_score[(int64_t)q * a.cap + slot] = v;
+              }
+            }
+          }
+      }
+    __syncthreads();     // stage is reloaded two tiles later
+    stage ^= 1;
+  }
+  cp_wait<0>();
+}
+
+// Dense scores [nq][n] of the codes (for threshold sampling): one CTA per
+// 128 queries x 128 rows.
+__global__ void __launch_bounds__(GEMM_THREADS) score_dense_kernel(SelArgs a, float* out) {
+  extern __shared__ __align__(16) unsigned char ssm[];
+  uint8_t* sQ = ssm;
+  uint8_t* sD = ssm + 128 * SLD;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int q0 = blockIdx.y * 128;
+  const int64_t r0 = (int64_t)blockIdx.x * 128;
+  for (int c = tid; c < 128 * (SK / 16); c += GEMM_THREADS) {
+    const int r = c / (SK / 16), kc = (c % (SK / 16)) * 16;
+    const bool okq = q0 + r < a.nq;
+    cp_async16(sQ + r * SLD + kc, a.Q + (int64_t)(okq ? q0 + r : 0) * SK + kc, okq);
+    const bool okd = r0 + r < a.n;
+    cp_async16(sD + r * SLD + kc, a.DB + (okd ? r0 + r : 0) * SK + kc, okd);
+  }
+  cp_commit();
+  cp_wait<0>();
+  __syncthreads();
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+#pragma unroll
+  for (int ks = 0; ks < SK; ks += 32) {
+    uint32_t af[4][4], bf[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      ldsm_x4(af[i], sQ + (wm * 64 + i * 16 + (lane & 15)) * SLD + ks + (lane >> 4) * 16);
+#pragma unroll
+    for (int jp = 0; jp < 2; ++jp) {
+      uint32_t t[4];
+      const int j = lane >> 3, r = lane & 7;
+      ldsm_x4(t, sD + (wn * 32 + jp * 16 + (j >> 1) * 8 + r) * SLD + ks + (j & 1) * 16);
+      bf[2 * jp][0] = t[0];
+      bf[2 * jp][1] = t[1];
+      bf[2 * jp + 1][0] = t[2];
+      bf[2 * jp + 1][1] = t[3];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_e4m3(acc[i][j], af[i], bf[j][0], bf[j][1]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = q0 + wm * 64 + i * 16 + (lane >> 2) + h * 8;
+      if (q >= a.nq) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int64_t row = r0 + wn * 32 + j * 8 + (lane & 3) * 2 + e;
+          if (row < a.n) out[(int64_t)q * a.n + row] = acc[i][j][2 * h + e];
+        }
+    }
+}
+
+// Residue classes of sequences placed in the padded row layout: row
+// row0[s] + i holds the class (0..19 as ARNDCQEGHILKMFPSTWYV, 20 for any
+// other byte) of byte off[s] + i, i < len[s]; other rows are left as set
+// by the caller (255: padding).  One block per sequence.
+__global__ void layout_kernel(const uint8_t* ascii, const int64_t* off, const int32_t* len,
+                              const int64_t* row0, uint8_t* cls) {
+  const int s = blockIdx.x;
+  const int n = len[s];
+  const uint8_t* src = ascii + off[s];
+  uint8_t* dst = cls + row0[s];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = ascii_class(src[i]);
+}
+
+// Per row of x [rows][n]: the k-th largest value (k >= 1, k <= n <= 8192),
+// by a bitonic sort of the row in shared memory.
+constexpr int kKthMax = 8192;
+__global__ void __launch_bounds__(1024) kth_largest_kernel(const float* x, int n, int k,
+                                                           float* out) {
+  __shared__ float v[kKthMax];
+  const float* row = x + (int64_t)blockIdx.x * n;
+  int size = 1;
+  while (size < n) size <<= 1;
+  for (int i = threadIdx.x; i < size; i += blockDim.x) v[i] = i < n ? row[i] : -INFINITY;
+  __syncthreads();
+  for (int len = 2; len <= size; len <<= 1) {
+    for (int stride = len >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool desc = (i & len) == 0;     // descending runs first
+          const float a = v[i], b = v[j];
+          if (desc ? (a < b) : (a > b)) { v[i] = b; v[j] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = v[k - 1];
+}
+
+int grid_for(int64_t work, int threads) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((work + threads - 1) / threads,
+                                                    (int64_t)device_sm_count() * 16));
+}
+
+}  // namespace emb
+}  // namespace sseqs
+
+using namespace sseqs;
+using namespace sseqs::emb;
+
+extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_t K,
+                               const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
+                               int64_t ldc, void* C2, const float* bias, const void* aux,
+                               const uint8_t* row_mask, cudaStream_t stream) {
+  if (M < 0 || N < 0 || K < 0 || (K % BK) != 0) return SSEQS_ERR_ARG;
+  if (M == 0 || N == 0) return SSEQS_OK;
+  if (!A || !B || !C) return SSEQS_ERR_ARG;
+  // every 16-byte chunk the tiles load must be aligned
+  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  if (!al(A) || !al(B) || (lda % 8) != 0 || (ldb % 8) != 0) return SSEQS_ERR_ARG;
+  if (a_t && (M % 8) != 0) return SSEQS_ERR_ARG;
+  if (b_t && (N % 8) != 0) return SSEQS_ERR_ARG;
+  if (epilogue == EPI_BIAS_GELU && (!bias || !C2)) return SSEQS_ERR_ARG;
+  if (epilogue == EPI_GELU_GRAD && !aux) return SSEQS_ERR_ARG;
+  GemmArgs g{M, N, K, static_cast<const __nv_bfloat16*>(A), lda,
+             static_cast<const __nv_bfloat16*>(B), ldb, C, ldc,
+             static_cast<__nv_bfloat16*>(C2), bias, static_cast<const __nv_bfloat16*>(aux),
+             row_mask};
+  const int key = (a_t ? 8 : 0) | (b_t ? 4 : 0) | (epilogue & 3);
+  if (epilogue < 0 || epilogue > 3) return SSEQS_ERR_ARG;
+  switch (key) {
+    case 0: return launch_gemm<false, false, EPI_F32>(g, stream);
+    case 1: return launch_gemm<false, false, EPI_BF16>(g, stream);
+    case 2: return launch_gemm<false, false, EPI_BIAS_GELU>(g, stream);
+    case 3: return launch_gemm<false, false, EPI_GELU_GRAD>(g, stream);
+    case 8 | 4 | 0: return launch_gemm<true, true, EPI_F32>(g, stream);
+    default: return SSEQS_ERR_UNSUPPORTED;
+  }
+}
+
+extern "C" int sseqs_embed_lookup(const uint8_t* cls, int64_t P, const void* E, int D, void* X,
+                                  cudaStream_t stream) {
+  if (P < 0 || D <= 0 || (P > 0 && (!cls || !E || !X))) return SSEQS_ERR_ARG;
+  if (P == 0) return SSEQS_OK;
+  { embed_lookup_kernel<<<grid_for(P * D, 256), 256, 0, stream>>>(
+        cls, P, static_cast<const __nv_bfloat16*>(E), D, static_cast<__nv_bfloat16*>(X));
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_embed_grad(const uint8_t* cls, int64_t P, const void* dX, int D, float* dE,
+                                cudaStream_t stream) {
+  if (P < 0 || D <= 0 || (P > 0 && (!cls || !dX || !dE))) return SSEQS_ERR_ARG;
+  if (P == 0) return SSEQS_OK;
+  { embed_grad_kernel<<<grid_for(P * D, 256), 256, 0, stream>>>(
+        cls, P, static_cast<const __nv_bfloat16*>(dX), D, dE);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_pool_normalize(const void* Y, int D, const int64_t* start, const int32_t* len,
+                                    int n_seqs, float* pooled, float* emb, float* inv_norm,
+                                    cudaStream_t stream) {
+  if (n_seqs < 0 || D < 32 || D > 1024 || (D % 32) != 0) return SSEQS_ERR_ARG;
+  if (n_seqs == 0) return SSEQS_OK;
+  if (!Y || !start || !len || !pooled || !emb || !inv_norm) return SSEQS_ERR_ARG;
+  { pool_normalize_kernel<<<n_seqs, D, 0, stream>>>(static_cast<const __nv_bfloat16*>(Y), start,
+                                                    len, pooled, emb, inv_norm);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const int32_t* ib,
+                               const float* y, int64_t B, float* dE, float* loss, float* pred,
+                               cudaStream_t stream) {
+  if (B < 0 || D <= 0 || (B > 0 && (!emb || !ia || !ib || !y || !loss))) return SSEQS_ERR_ARG;
+  if (B == 0) return SSEQS_OK;
+  const int64_t threads = B * 32;
+  const int grid = (int)((threads + 255) / 256);
+  { pair_loss_kernel<<<grid, 256, 0, stream>>>(emb, D, ia, ib, y, B, dE, loss, pred);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_pool_backward(const float* emb, const float* dE, const float* inv_norm,
+                                   const int64_t* start, const int32_t* len, int n_seqs, int D,
+                                   const void* Z, void* dZ, cudaStream_t stream) {
+  if (n_seqs < 0 || D < 32 || D > 1024 || (D % 32) != 0) return SSEQS_ERR_ARG;
+  if (n_seqs == 0) return SSEQS_OK;
+  if (!emb || !dE || !inv_norm || !start || !len || !Z || !dZ) return SSEQS_ERR_ARG;
+  { pool_backward_kernel<<<n_seqs, D, 0, stream>>>(emb, dE, inv_norm, start, len,
+                                                   static_cast<const __nv_bfloat16*>(Z),
+                                                   static_cast<__nv_bfloat16*>(dZ));
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_bias_grad(const void* dZ, int64_t P, int D, float* db, cudaStream_t stream) {
+  if (P < 0 || D <= 0 || (P > 0 && (!dZ || !db))) return SSEQS_ERR_ARG;
+  if (P == 0) return SSEQS_OK;
+  const int chunks = (int)std::min<int64_t>(P, (int64_t)device_sm_count() * 4);
+  const dim3 grid(chunks, (D + 255) / 256);
+  { bias_grad_kernel<<<grid, 256, 0, stream>>>(static_cast<const __nv_bfloat16*>(dZ), P, D, db);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_adam_conv(float* w, float* m, float* v, const float* dWT, int Cout, int Cin,
+                               float lr, float b1, float b2, float eps, int step, void* Wb,
+                               void* Wf, cudaStream_t stream) {
+  if (Cout <= 0 || Cin <= 0 || step < 1 || !w || !m || !v || !dWT || !Wb || !Wf)
+    return SSEQS_ERR_ARG;
+  AdamArgs o{lr, b1, b2, eps, 1.f - powf(b1, (float)step), 1.f - powf(b2, (float)step)};
+  { adam_conv_kernel<<<grid_for((int64_t)Cout * 5 * Cin, 256), 256, 0, stream>>>(
+        w, m, v, dWT, Cout, Cin, o, static_cast<__nv_bfloat16*>(Wb),
+        static_cast<__nv_bfloat16*>(Wf));
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_adam_flat(float* w, float* m, float* v, const float* g, int64_t n, float lr,
+                               float b1, float b2, float eps, int step, void* wb,
+                               cudaStream_t stream) {
+  if (n < 0 || step < 1 || (n > 0 && (!w || !m || !v || !g))) return SSEQS_ERR_ARG;
+  if (n == 0) return SSEQS_OK;
+  AdamArgs o{lr, b1, b2, eps, 1.f - powf(b1, (float)step), 1.f - powf(b2, (float)step)};
+  { adam_flat_kernel<<<grid_for(n, 256), 256, 0, stream>>>(w, m, v, g, n, o,
+                                                          static_cast<__nv_bfloat16*>(wb));
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_quantize_e4m3(const float* x, int64_t n, float scale, uint8_t* out,
+                                   cudaStream_t stream) {
+  if (n < 0 || (n > 0 && (!x || !out))) return SSEQS_ERR_ARG;
+  if (n == 0) return SSEQS_OK;
+  { quantize_e4m3_kernel<<<grid_for(n, 256), 256, 0, stream>>>(x, n, scale, out);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+static size_t score_smem(int stages) { return (size_t)(1 + stages) * 128 * SLD; }
+
+extern "C" int sseqs_score_select(const uint8_t* Q, int nq, const uint8_t* DB, int64_t n,
+                                  const float* tau, int32_t* count, int64_t* cand,
+                                  float* cand_score, int cap, cudaStream_t stream) {
+  if (nq < 0 || n < 0 || cap < 0) return SSEQS_ERR_ARG;
+  if (nq == 0 || n == 0) return SSEQS_OK;
+  if (!Q || !DB || !tau || !count || !cand || !cand_score) return SSEQS_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(DB) & 15))
+    return SSEQS_ERR_ARG;
+  SelArgs a{Q, nq, DB, n, tau, count, cand, cand_score, cap};
+  const size_t smem = score_smem(2);
+  if (cudaFuncSetAttribute((const void*)score_select_kernel,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const int qt = (nq + 127) / 128;
+  const int64_t ntiles = (n + 127) / 128;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, score_select_kernel, GEMM_THREADS, smem) !=
+          cudaSuccess || nb < 1)
+    return SSEQS_ERR_CUDA;
+  const int64_t slots = (int64_t)device_sm_count() * nb;
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (slots + qt - 1) / qt));
+  { score_select_kernel<<<dim3(gx, qt), GEMM_THREADS, smem, stream>>>(a); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_score_dense(const uint8_t* Q, int nq, const uint8_t* DB, int64_t n,
+                                 float* out, cudaStream_t stream) {
+  if (nq < 0 || n < 0) return SSEQS_ERR_ARG;
+  if (nq == 0 || n == 0) return SSEQS_OK;
+  if (!Q || !DB || !out) return SSEQS_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(DB) & 15))
+    return SSEQS_ERR_ARG;
+  SelArgs a{Q, nq, DB, n, nullptr, nullptr, nullptr, nullptr, 0};
+  const size_t smem = score_smem(1);
+  if (cudaFuncSetAttribute((const void*)score_dense_kernel,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const int64_t gx = (n + 127) / 128;
+  if (gx > INT32_MAX) return SSEQS_ERR_UNSUPPORTED;
+  { score_dense_kernel<<<dim3((unsigned)gx, (nq + 127) / 128), GEMM_THREADS, smem, stream>>>(a, out);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_embed_layout(const uint8_t* ascii, const int64_t* off, const int32_t* len,
+                                  const int64_t* row0, int n_seqs, uint8_t* cls,
+                                  cudaStream_t stream) {
+  if (n_seqs < 0 || (n_seqs > 0 && (!ascii || !off || !len || !row0 || !cls)))
+    return SSEQS_ERR_ARG;
+  if (n_seqs == 0) return SSEQS_OK;
+  { layout_kernel<<<n_seqs, 128, 0, stream>>>(ascii, off, len, row0, cls); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+extern "C" int sseqs_kth_largest_rows(const float* x, int rows, int n, int k, float* out,
+                                      cudaStream_t stream) {
+  if (rows < 0 || n < 1 || n > kKthMax || k < 1 || k > n) return SSEQS_ERR_ARG;
+  if (rows == 0) return SSEQS_OK;
+  if (!x || !out) return SSEQS_ERR_ARG;
+  { kth_largest_kernel<<<rows, 1024, 0, stream>>>(x, n, k, out); count_launches(1); }
+  return status_of(cudaGetLastError());
+}

@@ -1,0 +1,516 @@
+"""Learned prefilter: a 1D-conv sequence embedder and an FP8 candidate search.
+
+The reference narrows the database with a gapless FFT correlation before
+exact SW (sseqs/msa.py:281-307).  This module offers a learned alternative
+for the same stage (it has no reference counterpart):
+
+* ``Embedder`` -- residue embedding (21 classes -> 32), four width-5
+  convolutions to 256 channels with GELU, mean over the sequence, L2
+  normalisation: 1.03M parameters.  Forward and backward run on the tensor
+  cores through ``sseqs_gemm_bf16`` (BF16 operands, fp32 accumulation) with
+  fused bias/GELU/mask epilogues; the optimiser is Adam on fp32 master
+  weights (``sseqs_adam_conv`` / ``sseqs_adam_flat``).
+* ``training_pairs`` / ``train`` -- the embedder learns the exact affine SW
+  score of (query, target) pairs divided by the query's self-score, on
+  seeded planted-homolog data whose scores come from this package's own SW
+  kernels (``batched.sw_scan_queries``); the loss is the squared error of
+  the embeddings' cosine.
+* ``LearnedIndex`` -- the embeddings of every database segment as FP8 e4m3
+  codes resident in HBM; a query's candidates are the rows whose code dot
+  product reaches a per-query threshold (estimated from a sample so that
+  about ``factor`` times the wanted count pass), selected inside the FP8
+  GEMM's epilogue (``sseqs_score_select``), cut to the wanted count, and
+  re-scored by exact affine SW.  Every reported score is an exact integer SW
+  score; recall against the exhaustive search is measured by the caller.
+"""
+from __future__ import annotations
+
+import importlib
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import select, tune
+from ._lib import check, lib, ptr, stream_ptr, to_host
+
+D = 256            # channels and embedding width
+E = 32             # residue embedding width
+NCLS = 21
+MAX_LEN = 2048     # residues of a sequence the embedder reads
+CODE_SCALE = 16.0  # FP8 codes hold 16 x the unit-norm embedding
+
+_EPI_F32, _EPI_BF16, _EPI_BIAS_GELU, _EPI_GELU_GRAD = 0, 1, 2, 3
+
+
+def _gemm(a_t, b_t, epi, M, N, K, A, lda, B, ldb, C, ldc, C2=None, bias=None, aux=None,
+          mask=None):
+    check(lib().sseqs_gemm_bf16(a_t, b_t, epi, M, N, K, A, lda, B, ldb, C, ldc, C2,
+                                ptr(bias), aux, ptr(mask), stream_ptr()), "gemm_bf16")
+
+
+@dataclass
+class Layout:
+    """Padded row layout of a set of sequences (see sseqs_embed_layout)."""
+    P: int
+    cls: torch.Tensor        # uint8 [P]
+    mask: torch.Tensor       # uint8 [P], 1 on residue rows
+    start: torch.Tensor      # int64 [S], first row of each sequence
+    length: torch.Tensor     # int32 [S]
+
+    @property
+    def n(self) -> int:
+        return self.start.numel()
+
+
+def make_layout(ascii: torch.Tensor, offsets: torch.Tensor, lengths: torch.Tensor,
+                max_len: int = MAX_LEN) -> Layout:
+    """Layout of the sequences ascii[offsets[s] : + lengths[s]] (device)."""
+    dev = ascii.device
+    L = lengths.to(torch.int64).clamp(0, max_len)
+    sizes = L + 2
+    row0 = torch.cumsum(sizes, 0) - sizes + 2
+    P = 2 + int(sizes.sum().item())
+    P = (P + 31) // 32 * 32
+    cls = torch.full((P,), 255, dtype=torch.uint8, device=dev)
+    n = L.numel()
+    L32 = L.to(torch.int32)
+    off = offsets.to(torch.int64).contiguous()
+    check(lib().sseqs_embed_layout(ptr(ascii), ptr(off), ptr(L32), ptr(row0), n, ptr(cls),
+                                   stream_ptr()), "embed_layout")
+    mask = (cls != 255).to(torch.uint8)
+    return Layout(P, cls, mask, row0, L32)
+
+
+class _Buffers:
+    """Activation buffers with 2 zero rows of slack on both sides."""
+
+    def __init__(self, rows: int, train: bool, dev):
+        self.rows = rows
+        z = lambda c: torch.zeros((rows + 4, c), dtype=torch.bfloat16, device=dev)
+        self.X0 = z(E)
+        self.Y = [z(D) for _ in range(4)]
+        self.Z = [z(D) for _ in range(4)] if train else [z(D)]
+        self.dZ = [z(D) for _ in range(4)] if train else None
+        self.dX0 = z(E) if train else None
+
+
+def _base(buf: torch.Tensor) -> int:
+    """Address of layout row 0 (buffer row 2)."""
+    return buf.data_ptr() + 2 * buf.shape[1] * buf.element_size()
+
+
+class Embedder:
+    """The 1D-conv embedder with its Adam state (all parameters on device)."""
+
+    def __init__(self, seed: int = 0, device="cuda"):
+        dev = torch.device(device)
+        self.device = dev
+        g = torch.Generator(device="cpu")
+        g.manual_seed(seed)
+        self.cin = [E, D, D, D]
+        self.emb = (torch.randn(NCLS, E, generator=g) * 0.5).to(dev)
+        self.W = [(torch.randn(D, 5, c, generator=g) * math.sqrt(2.0 / (5 * c))).to(dev)
+                  for c in self.cin]
+        self.b = [torch.zeros(D, device=dev) for _ in self.cin]
+        self._opt = None
+        self.step = 0
+        self._bufs = None
+        self._sync_bf16()
+
+    @property
+    def n_params(self) -> int:
+        return self.emb.numel() + sum(w.numel() + b.numel() for w, b in zip(self.W, self.b))
+
+    def _sync_bf16(self):
+        self.emb_b = self.emb.to(torch.bfloat16).contiguous()
+        self.Wb = [w.reshape(D, -1).to(torch.bfloat16).contiguous() for w in self.W]
+        self.Wf = [w.flip(1).permute(2, 1, 0).reshape(c, -1).to(torch.bfloat16).contiguous()
+                   for w, c in zip(self.W, self.cin)]
+
+    def state_dict(self) -> dict:
+        return {"emb": self.emb.cpu(), "W": [w.cpu() for w in self.W],
+                "b": [b.cpu() for b in self.b]}
+
+    def load_state_dict(self, st: dict):
+        self.emb = st["emb"].to(self.device)
+        self.W = [w.to(self.device) for w in st["W"]]
+        self.b = [b.to(self.device) for b in st["b"]]
+        self._sync_bf16()
+
+    def _buffers(self, rows: int, train: bool) -> _Buffers:
+        b = self._bufs
+        if b is None or b.rows < rows or (train and b.dZ is None):
+            self._bufs = None
+            torch.cuda.empty_cache()
+            b = self._bufs = _Buffers(max(rows, 1024), train, self.device)
+        return b
+
+    # ---------------------------------------------------------------- forward
+    def forward(self, lay: Layout, train: bool = False):
+        """Unit-norm embeddings [S, 256] (fp32) of the layout's sequences."""
+        bufs = self._buffers(lay.P, train)
+        P = lay.P
+        L = lib()
+        check(L.sseqs_embed_lookup(ptr(lay.cls), P, ptr(self.emb_b), E, _base(bufs.X0),
+                                   stream_ptr()), "embed_lookup")
+        prev, cprev = bufs.X0, E
+        for l in range(4):
+            Y = bufs.Y[l]
+            Z = bufs.Z[l] if train else bufs.Z[0]
+            # im2col(prev) row p starts at layout row p-2 = buffer row p
+            _gemm(0, 0, _EPI_BIAS_GELU, P, D, 5 * cprev, prev.data_ptr(), cprev,
+                  self.Wb[l].data_ptr(), 5 * cprev, _base(Y), D, _base(Z), self.b[l], None,
+                  lay.mask)
+            prev, cprev = Y, D
+        S = lay.n
+        pooled = torch.empty((S, D), dtype=torch.float32, device=self.device)
+        emb = torch.empty((S, D), dtype=torch.float32, device=self.device)
+        inv = torch.empty(S, dtype=torch.float32, device=self.device)
+        check(L.sseqs_pool_normalize(_base(prev), D, ptr(lay.start), ptr(lay.length), S,
+                                     ptr(pooled), ptr(emb), ptr(inv), stream_ptr()),
+              "pool_normalize")
+        if train:
+            self._cache = (lay, emb, inv)
+        return emb
+
+    # --------------------------------------------------------------- backward
+    def backward(self, dE: torch.Tensor):
+        """Gradients of every parameter from dLoss/d(embeddings) (after a
+        ``forward(..., train=True)``); returns them as a dict."""
+        lay, emb, inv = self._cache
+        bufs, P, L = self._bufs, lay.P, lib()
+        bufs.dZ[3][2:2 + P].zero_()
+        check(L.sseqs_pool_backward(ptr(emb), ptr(dE), ptr(inv), ptr(lay.start),
+                                    ptr(lay.length), lay.n, D, _base(bufs.Z[3]),
+                                    _base(bufs.dZ[3]), stream_ptr()), "pool_backward")
+        grads = {"W": [None] * 4, "b": [None] * 4}
+        for l in range(3, -1, -1):
+            cin = self.cin[l]
+            prev = bufs.Y[l - 1] if l > 0 else bufs.X0
+            dZ = bufs.dZ[l]
+            dWT = torch.empty((5 * cin, D), dtype=torch.float32, device=self.device)
+            # dW^T = im2col(prev)^T . dZ over the P rows
+            _gemm(1, 1, _EPI_F32, 5 * cin, D, P, prev.data_ptr(), cin, _base(dZ), D,
+                  dWT.data_ptr(), D)
+            db = torch.zeros(D, dtype=torch.float32, device=self.device)
+            check(L.sseqs_bias_grad(_base(dZ), P, D, ptr(db), stream_ptr()), "bias_grad")
+            grads["W"][l], grads["b"][l] = dWT, db
+            # data gradient through the transposed (flipped) kernel
+            if l > 0:
+                _gemm(0, 0, _EPI_GELU_GRAD, P, cin, 5 * D, dZ.data_ptr(), D,
+                      self.Wf[l].data_ptr(), 5 * D, _base(bufs.dZ[l - 1]), cin, None, None,
+                      _base(bufs.Z[l - 1]), lay.mask)
+            else:
+                _gemm(0, 0, _EPI_BF16, P, cin, 5 * D, dZ.data_ptr(), D, self.Wf[0].data_ptr(),
+                      5 * D, _base(bufs.dX0), cin, None, None, None, lay.mask)
+        dEmb = torch.zeros((NCLS, E), dtype=torch.float32, device=self.device)
+        check(L.sseqs_embed_grad(ptr(lay.cls), P, _base(bufs.dX0), E, ptr(dEmb), stream_ptr()),
+              "embed_grad")
+        grads["emb"] = dEmb
+        return grads
+
+    def apply(self, grads: dict, lr: float, b1=0.9, b2=0.999, eps=1e-8):
+        """One Adam step with the gradients of ``backward``."""
+        if self._opt is None:
+            z = lambda t: torch.zeros_like(t)
+            self._opt = {"emb": (z(self.emb), z(self.emb)),
+                         "W": [(z(w), z(w)) for w in self.W],
+                         "b": [(z(b), z(b)) for b in self.b]}
+        self.step += 1
+        L, st = lib(), stream_ptr()
+        for l in range(4):
+            m, v = self._opt["W"][l]
+            check(L.sseqs_adam_conv(ptr(self.W[l]), ptr(m), ptr(v), ptr(grads["W"][l]), D,
+                                    self.cin[l], lr, b1, b2, eps, self.step, ptr(self.Wb[l]),
+                                    ptr(self.Wf[l]), st), "adam_conv")
+            m, v = self._opt["b"][l]
+            check(L.sseqs_adam_flat(ptr(self.b[l]), ptr(m), ptr(v), ptr(grads["b"][l]), D, lr,
+                                    b1, b2, eps, self.step, None, st), "adam_flat")
+        m, v = self._opt["emb"]
+        check(L.sseqs_adam_flat(ptr(self.emb), ptr(m), ptr(v), ptr(grads["emb"]),
+                                self.emb.numel(), lr, b1, b2, eps, self.step, ptr(self.emb_b),
+                                st), "adam_flat")
+
+    def embed(self, ascii, offsets, lengths, chunk: int = 8192) -> torch.Tensor:
+        """Embeddings [n, 256] of many sequences, ``chunk`` at a time."""
+        n = lengths.numel()
+        out = torch.empty((n, D), dtype=torch.float32, device=self.device)
+        for s in range(0, n, chunk):
+            lay = make_layout(ascii, offsets[s:s + chunk], lengths[s:s + chunk])
+            out[s:s + lay.n] = self.forward(lay)
+        return out
+
+
+# ------------------------------------------------------------- training data
+@dataclass
+class PairSet:
+    """Sequences (queries and targets) in one byte buffer, and the pairs."""
+    ascii: torch.Tensor      # device bytes, sequences separated by '@'
+    offsets: torch.Tensor    # int64 [n_seqs]
+    lengths: torch.Tensor    # int32 [n_seqs]
+    qa: torch.Tensor         # int32 [B] query sequence of each pair
+    tb: torch.Tensor         # int32 [B] target sequence of each pair
+    y: torch.Tensor          # float32 [B]: SW(q, t) / SW(q, q)
+    n_queries: int
+    per_query: int
+
+
+def training_pairs(n_queries: int, per_query: int, seed: int = 0, ident=(0.15, 1.0),
+                   homolog_frac: float = 0.5, device="cuda", gap_open=11,
+                   gap_extend=1) -> PairSet:
+    """Seeded pairs: queries with lengths U(50, 1000); per query a fraction
+    ``homolog_frac`` of mutated copies (identity U(ident), indels) and
+    unrelated sequences (log-normal lengths, median 250) for the rest.  The
+    target of a pair is the exact affine SW score of (query, target) divided
+    by the query's self-score, computed with the score kernels."""
+    from . import batched, dbtools
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    qlens = rng.integers(50, 1001, n_queries)
+    nh = int(round(per_query * homolog_frac))
+    parts, lens = [], []
+    for qi in range(n_queries):
+        q = dbtools.random_residues(int(qlens[qi]), gen, dev)
+        parts.append(q)
+        lens.append(torch.tensor([q.numel()], device=dev))
+        qs = q.cpu().numpy().tobytes().decode()
+        res, ln = dbtools.plant_homologs(qs, nh, ident[0], ident[1], gen, dev)
+        parts.append(res)
+        lens.append(ln)
+        bl = dbtools.lognormal_lengths(per_query - nh, gen, dev)
+        parts.append(dbtools.random_residues(int(bl.sum().item()), gen, dev))
+        lens.append(bl)
+    lengths = torch.cat(lens).to(torch.int64)
+    residues = torch.cat(parts)
+    n = lengths.numel()
+    # interleave '@' after every sequence
+    offsets = torch.cumsum(lengths + 1, 0) - (lengths + 1)
+    ascii = torch.full((int((lengths + 1).sum().item()),), 64, dtype=torch.uint8, device=dev)
+    seq_of = torch.repeat_interleave(torch.arange(n, device=dev), lengths)
+    pos = torch.arange(residues.numel(), device=dev) - \
+        (torch.cumsum(lengths, 0) - lengths)[seq_of]
+    ascii[offsets[seq_of] + pos] = residues
+    delim = (offsets + lengths).to(torch.int32)
+    stride = 1 + per_query
+    qa = torch.arange(n_queries, device=dev).repeat_interleave(per_query) * stride
+    tb = qa + torch.arange(per_query, device=dev).repeat(n_queries) + 1
+    # exact scores: target g of segment index g (window between delim[g-1]
+    # and delim[g]); each query against [itself, its targets]
+    sw = importlib.import_module("sseqs_b200.sw")
+    scores = torch.empty((n_queries, stride), dtype=torch.int32, device=dev)
+    encs = [sw.encode_query(bytes(ascii[int(offsets[i * stride]):int(offsets[i * stride]) +
+                                        int(lengths[i * stride])].cpu().numpy()).decode(), dev)
+            for i in range(n_queries)]
+    for tpt, members in batched.buckets([e.numel() for e in encs]).items():
+        for s in range(0, len(members), batched.GROUP):
+            grp = members[s:s + batched.GROUP]
+            qbuf = torch.zeros((len(grp), batched.MAX_QUERY), dtype=torch.uint8, device=dev)
+            for j, qi in enumerate(grp):
+                qbuf[j, :encs[qi].numel()] = encs[qi]
+            ql = torch.tensor([encs[qi].numel() for qi in grp], dtype=torch.int32, device=dev)
+            idx = torch.stack([torch.arange(qi * stride, (qi + 1) * stride, device=dev)
+                               for qi in grp]).to(torch.int32)
+            out = batched.sw_scan_queries(qbuf, ql, tpt, ascii, delim, affine=True,
+                                          good_idx=idx, skip=0, gap_a=gap_open,
+                                          gap_b=gap_extend)
+            scores[torch.tensor(grp, device=dev)] = out[:, :stride]
+    self_s = scores[:, 0:1].clamp(min=1).to(torch.float32)
+    y = (scores[:, 1:].to(torch.float32) / self_s).clamp_(0, 1).flatten()
+    return PairSet(ascii, offsets, lengths.to(torch.int32), qa.to(torch.int32),
+                   tb.to(torch.int32), y, n_queries, per_query)
+
+
+def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
+          targets_per_query: int = 32, epochs: int = 1, lr: float = 2e-3,
+          lr_end: float = 1e-4, seed: int = 0, log=None) -> dict:
+    """Adam on the squared error between embedding cosines and the pairs'
+    normalised SW scores.  Each step takes ``queries_per_step`` queries and
+    ``targets_per_query`` of each one's targets."""
+    dev = model.device
+    rng = np.random.default_rng(seed)
+    nq, pq = pairs.n_queries, pairs.per_query
+    tq = min(targets_per_query, pq)
+    slices = [(q, t0) for q in range(nq) for t0 in range(0, pq - tq + 1, tq)]
+    total = epochs * (len(slices) // queries_per_step)
+    losses, step = [], 0
+    loss_acc = torch.zeros(1, dtype=torch.float32, device=dev)
+    stride = 1 + pq
+    for ep in range(epochs):
+        order = rng.permutation(len(slices))
+        for s0 in range(0, len(order) - queries_per_step + 1, queries_per_step):
+            pick = [slices[i] for i in order[s0:s0 + queries_per_step]]
+            seq = []
+            ia, ib, yy = [], [], []
+            for j, (q, t0) in enumerate(pick):
+                base = len(seq)
+                seq.append(q * stride)
+                seq.extend(range(q * stride + 1 + t0, q * stride + 1 + t0 + tq))
+                ia.extend([base] * tq)
+                ib.extend(range(base + 1, base + 1 + tq))
+                yy.append((q * pq + t0, tq))
+            sidx = torch.tensor(seq, dtype=torch.int64, device=dev)
+            lay = make_layout(pairs.ascii, pairs.offsets[sidx], pairs.lengths[sidx])
+            emb = model.forward(lay, train=True)
+            y = torch.cat([pairs.y[a:a + n] for a, n in yy])
+            ia_t = torch.tensor(ia, dtype=torch.int32, device=dev)
+            ib_t = torch.tensor(ib, dtype=torch.int32, device=dev)
+            dE = torch.zeros_like(emb)
+            loss_acc.zero_()
+            check(lib().sseqs_pair_loss(ptr(emb), D, ptr(ia_t), ptr(ib_t), ptr(y), ia_t.numel(),
+                                        ptr(dE), ptr(loss_acc), None, stream_ptr()), "pair_loss")
+            grads = model.backward(dE)
+            frac = step / max(total - 1, 1)
+            cur = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * frac))
+            model.apply(grads, cur)
+            if step % 50 == 0 or step == total - 1:
+                losses.append((step, float(loss_acc.item())))
+                if log:
+                    log(f"step {step}/{total} loss {losses[-1][1]:.5f} lr {cur:.2e}")
+            step += 1
+    return {"steps": step, "losses": losses}
+
+
+# ----------------------------------------------------------------- search
+class LearnedIndex:
+    """FP8 codes of every database segment, resident in HBM."""
+
+    def __init__(self, model: Embedder, db, chunk: int = 8192):
+        self.model, self.db = model, db
+        counts = [b.n_segments for b in db.batches]
+        self.cum = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        n = int(self.cum[-1])
+        self.codes = torch.empty((max(n, 1), D), dtype=torch.uint8, device=db.device)
+        L = lib()
+        for bi, b in enumerate(db.batches):
+            for s in range(0, b.n_segments, chunk):
+                e = min(s + chunk, b.n_segments)
+                emb = model.embed(b.ascii, b.offsets[s:e], b.lengths[s:e], chunk=chunk)
+                row = int(self.cum[bi]) + s
+                check(L.sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE,
+                                            self.codes[row:row + (e - s)].data_ptr(),
+                                            stream_ptr()), "quantize")
+        self.n = n
+
+    def query_codes(self, enc_queries) -> torch.Tensor:
+        """FP8 codes [nq, 256] of queries given as ASCII strings."""
+        dev = self.db.device
+        buf = "".join(q + "@" for q in enc_queries).encode()
+        ascii = torch.from_numpy(np.frombuffer(buf, np.uint8).copy()).to(dev)
+        lens = torch.tensor([len(q) for q in enc_queries], dtype=torch.int64, device=dev)
+        offs = torch.cumsum(lens + 1, 0) - (lens + 1)
+        emb = self.model.embed(ascii, offs, lens)
+        codes = torch.empty((len(enc_queries), D), dtype=torch.uint8, device=dev)
+        check(lib().sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE, ptr(codes),
+                                        stream_ptr()), "quantize")
+        return codes
+
+    def candidates(self, qcodes: torch.Tensor, n_cand: int, sample: int = 8192,
+                   factor: float = 2.5, cap_factor: int = 8):
+        """Per query the database rows of its ``n_cand`` highest code scores
+        (fewer when fewer pass the threshold); list of int64 tensors."""
+        dev = self.db.device
+        nq = qcodes.shape[0]
+        L = lib()
+        # threshold: the k-th largest score over an evenly spaced sample
+        S = min(sample, self.n)
+        rows = torch.linspace(0, self.n - 1, S, device=dev).round().to(torch.int64)
+        samp = self.codes[rows].contiguous()
+        dense = torch.empty((nq, S), dtype=torch.float32, device=dev)
+        check(L.sseqs_score_dense(ptr(qcodes), nq, ptr(samp), S, ptr(dense), stream_ptr()),
+              "score_dense")
+        k_s = max(1, min(S, int(math.ceil(factor * n_cand * S / max(self.n, 1)))))
+        tau = torch.empty(nq, dtype=torch.float32, device=dev)
+        check(L.sseqs_kth_largest_rows(ptr(dense), nq, S, k_s, ptr(tau), stream_ptr()),
+              "kth_largest")
+        cap = int(min(self.n, max(n_cand * cap_factor, 1024)))
+        while True:
+            count = torch.zeros(nq, dtype=torch.int32, device=dev)
+            cand = torch.empty((nq, cap), dtype=torch.int64, device=dev)
+            cs = torch.empty((nq, cap), dtype=torch.float32, device=dev)
+            check(L.sseqs_score_select(ptr(qcodes), nq, ptr(self.codes), self.n, ptr(tau),
+                                       ptr(count), ptr(cand), ptr(cs), cap, stream_ptr()),
+                  "score_select")
+            cnt = to_host(count)
+            if int(cnt.max(initial=0)) <= cap or cap >= self.n:
+                break
+            cap = int(min(self.n, 2 * int(cnt.max())))
+        out = []
+        for q in range(nq):
+            c = int(min(cnt[q], cap))
+            if c <= n_cand:
+                out.append(cand[q, :c])
+                continue
+            keys = cs[q, :c].to(torch.float16)
+            p = select.topk_indices(keys, n_cand).long()
+            out.append(cand[q, :c][p])
+        return out, cnt
+
+    def rescore(self, queries, cands, top: int = 4096, gap_open=11, gap_extend=1):
+        """Exact affine SW of every query against its candidate rows (the
+        affine stage of sseqs/msa.py:327-337: skip 1 residue, first and last
+        segment of a batch excluded); returns per query the ``top`` hits as
+        rows (normalised score, batch, segment, affine score) -- segment being
+        the delimiter-based index the exhaustive search reports -- sorted by
+        normalised score desc, then batch, then segment."""
+        from . import batched
+        sw = importlib.import_module("sseqs_b200.sw")
+        dev = self.db.device
+        enc = [sw.encode_query(q, device=dev) for q in queries]
+        results = [[] for _ in queries]
+        per_batch = []
+        for c in cands:
+            r = c.sort().values
+            cuts = torch.searchsorted(r, torch.tensor(self.cum, device=dev))
+            per_batch.append((r, cuts))
+        for bi, b in enumerate(self.db.batches):
+            lists = []
+            for qi, (r, cuts) in enumerate(per_batch):
+                f = r[int(cuts[bi]):int(cuts[bi + 1])] - int(self.cum[bi])
+                f = f[(f >= 1) & (f <= b.n_segments - 2)]
+                lists.append(f)
+            for tpt, members in batched.buckets([e.numel() for e in enc]).items():
+                for s in range(0, len(members), batched.GROUP):
+                    grp = [qi for qi in members[s:s + batched.GROUP] if lists[qi].numel()]
+                    if not grp:
+                        continue
+                    m = max(lists[qi].numel() for qi in grp)
+                    idx = torch.empty((len(grp), m), dtype=torch.int32, device=dev)
+                    for j, qi in enumerate(grp):
+                        f = lists[qi]
+                        g = b.seg_index[f].to(torch.int32)
+                        idx[j, :g.numel()] = g
+                        idx[j, g.numel():] = g[-1]
+                    qbuf = torch.zeros((len(grp), batched.MAX_QUERY), dtype=torch.uint8,
+                                       device=dev)
+                    for j, qi in enumerate(grp):
+                        qbuf[j, :enc[qi].numel()] = enc[qi]
+                    ql = torch.tensor([enc[qi].numel() for qi in grp], dtype=torch.int32,
+                                      device=dev)
+                    sc = batched.sw_scan_queries(qbuf, ql, tpt, b.ascii, b.delim, affine=True,
+                                                 good_idx=idx, skip=1, gap_a=gap_open,
+                                                 gap_b=gap_extend)
+                    for j, qi in enumerate(grp):
+                        n = lists[qi].numel()
+                        g = to_host(b.seg_index[lists[qi]].to(torch.int32))
+                        results[qi].append((bi, g, to_host(sc[j, :n]), b.maxlen))
+        out = []
+        for qi, q in enumerate(queries):
+            rows = []
+            Lq = len(q)
+            for bi, f, s, maxlen in results[qi]:
+                norm = (s.astype(np.float32) / np.sqrt(np.float32(Lq * maxlen))).astype(
+                    np.float32)
+                for k in range(f.size):
+                    rows.append((float(norm[k]), bi, int(f[k]), int(s[k])))
+            rows.sort(key=lambda x: (-x[0], x[1], x[2]))
+            out.append(rows[:top])
+        return out
+
+    def search(self, queries, n_cand: int = 32768, top: int = 4096, **kw):
+        codes = self.query_codes(queries)
+        cands, _ = self.candidates(codes, n_cand, **kw)
+        return self.rescore(queries, cands, top=top)

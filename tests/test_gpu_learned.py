@@ -1,0 +1,210 @@
+"""GPU tests of the learned prefilter's kernels against plain PyTorch fp32
+references of the same operations (tolerances stated per test), and of the
+search's contract: every reported score is the exact SW score."""
+import importlib
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf(x):
+    return x.to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 32), (300, 200, 160), (1000, 256, 1280),
+                                   (77, 32, 64)])
+@pytest.mark.parametrize("epi", [0, 1, 2, 3])
+def test_gemm_nt_matches_fp32(M, N, K, epi):
+    from sseqs_b200 import learned
+    g = torch.Generator(device="cpu")
+    g.manual_seed(M + N + K + epi)
+    A = _bf(torch.randn(M, K, generator=g)).cuda()
+    B = _bf(torch.randn(N, K, generator=g)).cuda()
+    bias = torch.randn(N, generator=g).cuda()
+    aux = _bf(torch.randn(M, N, generator=g)).cuda()
+    mask = (torch.rand(M, generator=g) > 0.2).to(torch.uint8).cuda()
+    ref = A.float() @ B.float().T
+    C = torch.zeros((M, N), dtype=torch.float32 if epi == 0 else torch.bfloat16, device="cuda")
+    C2 = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda")
+    learned._gemm(0, 0, epi, M, N, K, A.data_ptr(), K, B.data_ptr(), K, C.data_ptr(), N,
+                  C2.data_ptr(), bias, aux.data_ptr(), mask if epi else None)
+    m = mask.bool()[:, None]
+    if epi == 0:
+        exp = ref
+    elif epi == 1:
+        exp = torch.where(m, ref, 0)
+    elif epi == 2:
+        z = _bf(ref + bias).float()
+        assert torch.allclose(C2.float(), torch.where(m, z, 0), rtol=1e-2, atol=1e-2)
+        exp = torch.where(m, torch.nn.functional.gelu(z, approximate="tanh"), 0)
+    else:
+        zf = aux.float()
+        t = torch.tanh(0.7978845608 * (zf + 0.044715 * zf ** 3))
+        gp = 0.5 * (1 + t) + 0.5 * zf * (1 - t * t) * 0.7978845608 * (1 + 0.134145 * zf * zf)
+        exp = torch.where(m, ref * gp, 0)
+    # fp32 accumulation of exact bf16 products; bf16 output rounding
+    tol = 1e-3 if epi == 0 else 1e-2
+    err = (C.float() - exp).abs().max().item()
+    assert err <= tol * max(1.0, exp.abs().max().item()), err
+
+
+@pytest.mark.parametrize("M,N,K", [(160, 256, 96), (1280, 256, 4096), (40, 24, 32)])
+def test_gemm_tn_matches_fp32(M, N, K):
+    from sseqs_b200 import learned
+    g = torch.Generator(device="cpu")
+    g.manual_seed(M * N + K)
+    A = _bf(torch.randn(K, M, generator=g)).cuda()      # stored [K][M]
+    B = _bf(torch.randn(K, N, generator=g)).cuda()      # stored [K][N]
+    C = torch.zeros((M, N), dtype=torch.float32, device="cuda")
+    learned._gemm(1, 1, 0, M, N, K, A.data_ptr(), M, B.data_ptr(), N, C.data_ptr(), N)
+    ref = A.float().T @ B.float()
+    assert (C - ref).abs().max().item() <= 1e-3 * ref.abs().max().item()
+
+
+def _ref_embed(model, seqs):
+    """fp32 reference: per sequence conv1d (padding 2) + GELU(tanh), mean,
+    L2 normalise, with the model's bf16-rounded parameters."""
+    from sseqs_b200 import sw as _unused  # noqa: F401
+    AA = "ARNDCQEGHILKMFPSTWYV"
+    E = model.emb_b.float()
+    outs = []
+    for s in seqs:
+        cls = torch.tensor([AA.index(c) if c in AA else 20 for c in s], device="cuda")
+        x = E[cls].T[None]                                  # [1, 32, L]
+        for l in range(4):
+            w = model.Wb[l].float().reshape(256, 5, -1).permute(0, 2, 1)   # [co, ci, 5]
+            x = torch.nn.functional.conv1d(x, w, model.b[l], padding=2)
+            x = torch.nn.functional.gelu(x, approximate="tanh")
+        p = x[0].mean(1)
+        outs.append(p / p.norm())
+    return torch.stack(outs)
+
+
+def _layout_of(seqs):
+    from sseqs_b200 import learned
+    buf = "".join(s + "@" for s in seqs).encode()
+    ascii = torch.from_numpy(np.frombuffer(buf, np.uint8).copy()).cuda()
+    lens = torch.tensor([len(s) for s in seqs], dtype=torch.int64, device="cuda")
+    offs = torch.cumsum(lens + 1, 0) - (lens + 1)
+    return learned.make_layout(ascii, offs, lens)
+
+
+def test_embedder_forward_matches_fp32_conv():
+    from sseqs_b200 import dbtools, learned
+    model = learned.Embedder(seed=3)
+    seqs = [dbtools.random_query(int(n), 40 + i) for i, n in enumerate([1, 5, 37, 300, 1000])]
+    seqs[3] = seqs[3][:20] + "XBZU" + seqs[3][24:]
+    got = model.forward(_layout_of(seqs))
+    exp = _ref_embed(model, seqs)
+    # bf16 activations between layers: cosine of the unit vectors >= 0.999
+    cos = (got * exp).sum(1)
+    assert bool((cos > 0.999).all()), cos
+
+
+def test_embedder_backward_matches_autograd():
+    from sseqs_b200 import dbtools, learned
+    model = learned.Embedder(seed=5)
+    seqs = [dbtools.random_query(int(n), 60 + i) for i, n in enumerate([50, 120, 80, 200])]
+    lay = _layout_of(seqs)
+    emb = model.forward(lay, train=True)
+    # loss = sum_s <emb_s, r_s> for a fixed random r: dE = r
+    g = torch.Generator(device="cpu")
+    g.manual_seed(9)
+    r = torch.randn(emb.shape, generator=g).cuda()
+    grads = model.backward(r.contiguous())
+    # reference with autograd on fp32 copies of the bf16 parameters
+    AA = "ARNDCQEGHILKMFPSTWYV"
+    Ep = model.emb_b.float().clone().requires_grad_()
+    Ws = [model.Wb[l].float().reshape(256, 5, -1).clone().requires_grad_() for l in range(4)]
+    bs = [model.b[l].clone().requires_grad_() for l in range(4)]
+    tot = 0
+    for si, s in enumerate(seqs):
+        cls = torch.tensor([AA.index(c) if c in AA else 20 for c in s], device="cuda")
+        x = Ep[cls].T[None]
+        for l in range(4):
+            x = torch.nn.functional.conv1d(x, Ws[l].permute(0, 2, 1), bs[l], padding=2)
+            x = torch.nn.functional.gelu(x, approximate="tanh")
+        p = x[0].mean(1)
+        tot = tot + ((p / p.norm()) * r[si]).sum()
+    tot.backward()
+
+    def close(a, b):   # bf16 forward/backward activations: cosine >= 0.99
+        a, b = a.flatten().float(), b.flatten().float()
+        return (a @ b / (a.norm() * b.norm() + 1e-30)).item()
+
+    for l in range(4):
+        cin = model.cin[l]
+        dW = grads["W"][l].reshape(5, cin, 256).permute(2, 0, 1)     # [co, t, ci]
+        assert close(dW, Ws[l].grad) > 0.99, l
+        assert close(grads["b"][l], bs[l].grad) > 0.99, l
+    assert close(grads["emb"], Ep.grad) > 0.99
+
+
+def test_score_select_and_threshold():
+    from sseqs_b200 import _lib, learned
+    g = torch.Generator(device="cpu")
+    g.manual_seed(1)
+    nq, n = 130, 5000
+    q = torch.randn(nq, 256, generator=g)
+    d = torch.randn(n, 256, generator=g)
+    q = (q / q.norm(dim=1, keepdim=True)).cuda()
+    d = (d / d.norm(dim=1, keepdim=True)).cuda()
+    L = _lib.lib()
+    qc = torch.empty((nq, 256), dtype=torch.uint8, device="cuda")
+    dc = torch.empty((n, 256), dtype=torch.uint8, device="cuda")
+    _lib.check(L.sseqs_quantize_e4m3(q.data_ptr(), q.numel(), 16.0, qc.data_ptr(), 0), "q")
+    _lib.check(L.sseqs_quantize_e4m3(d.data_ptr(), d.numel(), 16.0, dc.data_ptr(), 0), "q")
+    qf = qc.view(torch.float8_e4m3fn).float()
+    df = dc.view(torch.float8_e4m3fn).float()
+    ref = qf @ df.T                                             # fp32 reference
+    dense = torch.empty((nq, n), dtype=torch.float32, device="cuda")
+    _lib.check(L.sseqs_score_dense(qc.data_ptr(), nq, dc.data_ptr(), n, dense.data_ptr(), 0), "d")
+    assert (dense - ref).abs().max().item() < 1e-3
+    tau = torch.quantile(ref, 0.99, dim=1).contiguous()
+    cap = 200
+    cnt = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    cand = torch.empty((nq, cap), dtype=torch.int64, device="cuda")
+    cs = torch.empty((nq, cap), dtype=torch.float32, device="cuda")
+    _lib.check(L.sseqs_score_select(qc.data_ptr(), nq, dc.data_ptr(), n, tau.data_ptr(),
+                                    cnt.data_ptr(), cand.data_ptr(), cs.data_ptr(), cap, 0), "s")
+    for i in range(nq):
+        c = int(cnt[i])
+        assert c <= cap
+        got = set(cand[i, :c].tolist())
+        sure_in = set(torch.nonzero(ref[i] >= tau[i] + 1e-3).flatten().tolist())
+        maybe = set(torch.nonzero(ref[i] >= tau[i] - 1e-3).flatten().tolist())
+        assert sure_in <= got <= maybe
+    k = 7
+    kth = torch.empty(nq, dtype=torch.float32, device="cuda")
+    sub = ref[:, :4000].contiguous()
+    _lib.check(L.sseqs_kth_largest_rows(sub.data_ptr(), nq, 4000, k, kth.data_ptr(), 0), "k")
+    assert torch.equal(kth, torch.topk(sub, k, dim=1).values[:, -1])
+
+
+def test_learned_search_reports_exact_scores():
+    from sseqs_b200 import dbtools, learned, select
+    from sseqs_b200.database import Database
+    sw = importlib.import_module("sseqs_b200.sw")
+    pairs = learned.training_pairs(24, 32, seed=2)
+    model = learned.Embedder(seed=2)
+    hist = learned.train(model, pairs, queries_per_step=8, targets_per_query=16, epochs=2)
+    assert hist["losses"][-1][1] < hist["losses"][0][1]
+    q0 = dbtools.random_query(220, 11)
+    syn = dbtools.synthetic_db([q0], 4000, 0.02, (0.5, 0.95), seed=11, device="cpu",
+                               chunk_bytes=150_000)
+    db = Database(syn.chunks, bs=150_000)
+    idx = learned.LearnedIndex(model, db, chunk=1000)
+    hits = idx.search([q0], n_cand=300, top=50)[0]
+    assert hits
+    enc = sw.encode_query(q0)
+    for norm, bi, g, score in hits:
+        b = db.batches[bi]
+        exp = sw.sw_scan(enc, b.ascii, b.delim, affine=True,
+                         good_idx=torch.tensor([g], dtype=torch.int32, device="cuda"),
+                         skip=1, gap_a=11, gap_b=1)
+        assert int(exp[0]) == score
+        assert abs(norm - score / math.sqrt(len(q0) * b.maxlen)) < 1e-5
