@@ -291,6 +291,68 @@ def serving_leg(db, n_requests, rate, seed=4):
             "lengths": "U(50, 1000), seed %d" % seed}
 
 
+def learned_leg(db, exact_rows, n_pairs, n_queries, seed=5):
+    """Learned prefilter: train the conv embedder on ``n_pairs`` seeded
+    (query, target) pairs labelled by this package's exact SW, embed every
+    database segment into FP8 codes, then per query take 32768 candidates by
+    the FP8 GEMM, re-score them by exact affine SW, keep the top 4096 and
+    align them (the same tail as the exact step).  Queries/s over
+    ``n_queries`` queries U(50, 1000) (the exact leg's timed queries first);
+    recall of the exact search's top-1000 over the exact leg's queries."""
+    import torch
+    from sseqs_b200 import dbtools, learned
+    from sseqs_b200.to_a3m import align_all
+    per_query = 256
+    t0 = time.time()
+    pairs = learned.training_pairs(max(1, n_pairs // per_query), per_query, seed=seed)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    model = learned.Embedder(seed=seed)
+    hist = learned.train(model, pairs, epochs=1, seed=seed)
+    torch.cuda.synchronize()
+    t2 = time.time()
+    index = learned.LearnedIndex(model, db)
+    torch.cuda.synchronize()
+    t3 = time.time()
+    rng = np.random.default_rng(seed)
+    qs = list(exact_rows)
+    qs += [dbtools.random_query(int(L), 7000 + i)
+           for i, L in enumerate(rng.integers(50, 1001, max(0, n_queries - len(qs))))]
+
+    def step(batch_q):
+        res = index.search(batch_q, n_cand=32768, top=TOP_K)
+        for q, rows in zip(batch_q, res):
+            align_all(q, learned.hit_strings(db, rows))
+        return res
+
+    step(qs[:2])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = step(qs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    rec = []
+    for q, rows in zip(qs, res):
+        ex = exact_rows.get(q)
+        if not ex:
+            continue
+        want = {(r[1], r[2]) for r in ex[:1000]}
+        got = {(r[1], r[2]) for r in rows[:1000]}
+        rec.append(len(want & got) / max(1, len(want)))
+    return {"queries": len(qs), "queries_per_s": round(len(qs) / (ms * 1e-3), 3),
+            "ms_per_query": round(ms / len(qs), 2),
+            "recall_of_exact_top1000": round(float(np.mean(rec)), 4) if rec else None,
+            "recall_min": round(float(np.min(rec)), 4) if rec else None,
+            "recall_queries": len(rec), "candidates_per_query": 32768,
+            "train_pairs": int(pairs.y.numel()), "train_steps": hist["steps"],
+            "train_loss_first_last": [hist["losses"][0][1], hist["losses"][-1][1]],
+            "params": model.n_params, "seconds_pairs": round(t1 - t0, 1),
+            "seconds_train": round(t2 - t1, 1), "seconds_index": round(t3 - t2, 1),
+            "index_rows": index.n, "index_bytes": int(index.codes.numel())}
+
+
 def measured_peak(name):
     """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
     int pipes), in int16x2 lane-instructions per second."""
@@ -495,6 +557,10 @@ def bench_b200(args):
         out["batched"] = batched_leg(db, args.batched_queries)
     if world == 1 and args.serve_requests > 0:
         out["serving"] = serving_leg(db, args.serve_requests, args.serve_rate)
+    if world == 1 and args.learned_pairs > 0:
+        out["learned"] = learned_leg(db, exact_rows, args.learned_pairs, args.learned_queries)
+        out["learned"]["speedup_vs_exact_step"] = round(
+            out["learned"]["queries_per_s"] / out["queries_per_s"], 2)
     if world == 1 and not args.no_cpu_baseline:
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
@@ -563,6 +629,10 @@ def main():
                     help="requests of the serving leg; 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=1.5,
                     help="Poisson arrival rate (queries/s) of the serving leg")
+    ap.add_argument("--learned-pairs", type=int, default=1_000_000,
+                    help="training pairs of the learned-prefilter leg; 0 skips it")
+    ap.add_argument("--learned-queries", type=int, default=64,
+                    help="queries timed in the learned-prefilter leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

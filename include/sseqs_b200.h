@@ -251,10 +251,12 @@ int sseqs_sw_variant_words(int affine, int tpt, int wide);
 
 /* C = op(A) . op(B)^T over K (K % 32 == 0): A is [M x K] (a_t = 0, row
  * stride lda) or stored [K x M] (a_t = 1); B is [N x K] (b_t = 0) or
- * stored [K x N] (b_t = 1); supported (a_t, b_t): (0, 0) with every
- * epilogue, (1, 1) with epilogue 0.  Epilogue 0: C fp32; 1: C bf16;
+ * stored [K x N] (b_t = 1); supported (a_t, b_t): (0, 0) with epilogues
+ * 0-3, (1, 1) with epilogues 0 and 4.  Epilogue 0: C fp32; 1: C bf16;
  * 2: C2 = acc + bias (bf16 pre-activation), C = GELU(C2) (bf16, tanh form);
- * 3: C = acc * GELU'(aux) (bf16, aux bf16 with C's stride).  row_mask
+ * 3: C = acc * GELU'(aux) (bf16, aux bf16 with C's stride); 4: C (fp32,
+ * zeroed by the caller) += acc with K split over CTAs (for small M x N and
+ * long K, as in weight gradients).  row_mask
  * (nullable, uint8 per row of C): rows with 0 are written as 0 (epilogues
  * 1-3).  A, B 16-byte aligned, lda, ldb multiples of 8; a_t needs M % 8 ==
  * 0, b_t N % 8 == 0.  Tensor cores (mma.sync bf16, fp32 accumulation). */
@@ -278,12 +280,13 @@ int sseqs_embed_grad(const uint8_t* cls, int64_t P, const void* dX, int D, float
 int sseqs_pool_normalize(const void* Y, int D, const int64_t* start, const int32_t* len,
                          int n_seqs, float* pooled, float* emb, float* inv_norm,
                          cudaStream_t stream);
-/* For B pairs: pred = <emb[ia], emb[ib]>, *loss += (pred - y)^2 / B, and
- * (dE non-null) dE[ia] += 2 (pred - y) / B * emb[ib], dE[ib] likewise;
- * pred (nullable) receives the dot products. */
+/* For B pairs with weights w (weight nullable: 1/B each): pred =
+ * <emb[ia], emb[ib]>, *loss += w (pred - y)^2, and (dE non-null) dE[ia] +=
+ * 2 w (pred - y) emb[ib], dE[ib] likewise; pred (nullable) receives the dot
+ * products. */
 int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const int32_t* ib,
-                    const float* y, int64_t B, float* dE, float* loss, float* pred,
-                    cudaStream_t stream);
+                    const float* y, const float* weight, int64_t B, float* dE, float* loss,
+                    float* pred, cudaStream_t stream);
 /* Gradient of pool_normalize back to the last layer's pre-activation Z:
  * dZ[row] = (dE - emb <emb, dE>) * inv_norm / len * GELU'(Z[row]) for the
  * rows of every sequence (other rows untouched). */

@@ -57,7 +57,7 @@ _SIGNATURES = {
     "sseqs_embed_lookup": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_embed_grad": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_pool_normalize": (_I, [_P, _I, _P, _P, _I, _P, _P, _P, _P]),
-    "sseqs_pair_loss": (_I, [_P, _I, _P, _P, _P, _I64, _P, _P, _P, _P]),
+    "sseqs_pair_loss": (_I, [_P, _I, _P, _P, _P, _P, _I64, _P, _P, _P, _P]),
     "sseqs_pool_backward": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P]),
     "sseqs_bias_grad": (_I, [_P, _I64, _I, _P, _P]),
     "sseqs_adam_conv": (_I, [_P, _P, _P, _P, _I, _I, _F, _F, _F, _F, _I, _P, _P, _P]),

@@ -44,6 +44,7 @@ enum Epi : int {
   EPI_BF16 = 1,         // C (bf16) = acc  (masked rows -> 0)
   EPI_BIAS_GELU = 2,    // Z = acc + bias (bf16, C2), C = gelu(Z) (bf16); masked rows -> 0
   EPI_GELU_GRAD = 3,    // C (bf16) = acc * gelu'(aux);  masked rows -> 0
+  EPI_F32_ADD = 4,      // C (fp32) += acc (atomic; split-K partial sums)
 };
 
 __device__ __forceinline__ float gelu_f(float z) {
@@ -112,10 +113,15 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3;          // 2 x 4 warps of 64 x 32
   const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
-  const int64_t ktiles = g.K / BK;
+  // split-K: blockIdx.z takes k tiles [kt_lo, kt_hi)
+  const int64_t kt_all = g.K / BK;
+  const int64_t kt_per = (kt_all + gridDim.z - 1) / gridDim.z;
+  const int64_t kt_lo = (int64_t)blockIdx.z * kt_per;
+  const int64_t kt_hi = kt_lo + kt_per < kt_all ? kt_lo + kt_per : kt_all;
+  const int64_t ktiles = kt_hi > kt_lo ? kt_hi - kt_lo : 0;
 
   auto load_tile = [&](int stage, int64_t kt) {
-    const int64_t k0 = kt * BK;
+    const int64_t k0 = (kt_lo + kt) * BK;
     __nv_bfloat16* a = sA + stage * A_TILE;
     __nv_bfloat16* b = sB + stage * B_TILE;
 #pragma unroll
@@ -221,6 +227,10 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
           float* c = reinterpret_cast<float*>(g.C) + m * g.ldc + n;
           c[0] = v0;
           if (two) c[1] = v1;
+        } else if (EPI == EPI_F32_ADD) {
+          float* c = reinterpret_cast<float*>(g.C) + m * g.ldc + n;
+          atomicAdd(c, v0);
+          if (two) atomicAdd(c + 1, v1);
         } else if (EPI == EPI_BF16) {
           if (!keep) v0 = v1 = 0.f;
           __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
@@ -250,7 +260,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
 }
 
 template <bool A_T, bool B_T, int EPI>
-int launch_gemm(const GemmArgs& g, cudaStream_t stream) {
+int launch_gemm(const GemmArgs& g, cudaStream_t stream, int splits = 1) {
   constexpr int A_TILE = A_T ? BK * LDR : BM * LDK;
   constexpr int B_TILE = B_T ? BK * LDR : BN * LDK;
   constexpr size_t smem = sizeof(__nv_bfloat16) * STAGES * (A_TILE + B_TILE);
@@ -258,8 +268,9 @@ int launch_gemm(const GemmArgs& g, cudaStream_t stream) {
   if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return SSEQS_ERR_CUDA;
-  const dim3 grid((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM));
-  if (grid.y > 65535u) return SSEQS_ERR_UNSUPPORTED;
+  const dim3 grid((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM),
+                  (unsigned)splits);
+  if (grid.y > 65535u || grid.z > 65535u) return SSEQS_ERR_UNSUPPORTED;
   { fn<<<grid, GEMM_THREADS, smem, stream>>>(g); count_launches(1); }
   return status_of(cudaGetLastError());
 }
@@ -317,11 +328,12 @@ __global__ void pool_normalize_kernel(const __nv_bfloat16* Y, const int64_t* sta
   if (c == 0) inv_norm[s] = inv;
 }
 
-// One warp per pair: pred = <e_a, e_b>; loss += (pred - y)^2 / B;
-// dE_a += 2 (pred - y) / B * e_b, dE_b likewise.
+// One warp per pair: pred = <e_a, e_b>; with weight w (1/B when no
+// weights are given) loss += w (pred - y)^2, dE_a += 2 w (pred - y) e_b,
+// dE_b likewise.
 __global__ void pair_loss_kernel(const float* emb, int D, const int32_t* ia, const int32_t* ib,
-                                 const float* y, int64_t B, float* dE, float* loss,
-                                 float* pred_out) {
+                                 const float* y, const float* wt, int64_t B, float* dE,
+                                 float* loss, float* pred_out) {
   const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= B) return;
@@ -331,9 +343,10 @@ __global__ void pair_loss_kernel(const float* emb, int D, const int32_t* ia, con
   for (int c = lane; c < D; c += 32) d += ea[c] * eb[c];
   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
   const float r = d - y[w];
-  const float g = 2.f * r / (float)B;
+  const float wgt = wt ? wt[w] : 1.f / (float)B;
+  const float g = 2.f * r * wgt;
   if (lane == 0) {
-    atomicAdd(loss, r * r / (float)B);
+    atomicAdd(loss, r * r * wgt);
     if (pred_out) pred_out[w] = d;
   }
   if (dE) {
@@ -686,12 +699,21 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
   if (b_t && (N % 8) != 0) return SSEQS_ERR_ARG;
   if (epilogue == EPI_BIAS_GELU && (!bias || !C2)) return SSEQS_ERR_ARG;
   if (epilogue == EPI_GELU_GRAD && !aux) return SSEQS_ERR_ARG;
+  if (epilogue < 0 || epilogue > 4) return SSEQS_ERR_ARG;
   GemmArgs g{M, N, K, static_cast<const __nv_bfloat16*>(A), lda,
              static_cast<const __nv_bfloat16*>(B), ldb, C, ldc,
              static_cast<__nv_bfloat16*>(C2), bias, static_cast<const __nv_bfloat16*>(aux),
              row_mask};
+  if (epilogue == EPI_F32_ADD) {
+    // split K so that the grid covers every SM twice (C holds the sum of
+    // the partial products; the caller zeroes it)
+    if (a_t != 1 || b_t != 1) return SSEQS_ERR_UNSUPPORTED;
+    const int64_t tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    const int64_t want = (2 * (int64_t)device_sm_count() + tiles - 1) / tiles;
+    const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(want, K / BK));
+    return launch_gemm<true, true, EPI_F32_ADD>(g, stream, splits);
+  }
   const int key = (a_t ? 8 : 0) | (b_t ? 4 : 0) | (epilogue & 3);
-  if (epilogue < 0 || epilogue > 3) return SSEQS_ERR_ARG;
   switch (key) {
     case 0: return launch_gemm<false, false, EPI_F32>(g, stream);
     case 1: return launch_gemm<false, false, EPI_BF16>(g, stream);
@@ -735,13 +757,13 @@ extern "C" int sseqs_pool_normalize(const void* Y, int D, const int64_t* start, 
 }
 
 extern "C" int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const int32_t* ib,
-                               const float* y, int64_t B, float* dE, float* loss, float* pred,
-                               cudaStream_t stream) {
+                               const float* y, const float* weight, int64_t B, float* dE,
+                               float* loss, float* pred, cudaStream_t stream) {
   if (B < 0 || D <= 0 || (B > 0 && (!emb || !ia || !ib || !y || !loss))) return SSEQS_ERR_ARG;
   if (B == 0) return SSEQS_OK;
   const int64_t threads = B * 32;
   const int grid = (int)((threads + 255) / 256);
-  { pair_loss_kernel<<<grid, 256, 0, stream>>>(emb, D, ia, ib, y, B, dE, loss, pred);
+  { pair_loss_kernel<<<grid, 256, 0, stream>>>(emb, D, ia, ib, y, weight, B, dE, loss, pred);
     count_launches(1); }
   return status_of(cudaGetLastError());
 }

@@ -41,7 +41,7 @@ NCLS = 21
 MAX_LEN = 2048     # residues of a sequence the embedder reads
 CODE_SCALE = 16.0  # FP8 codes hold 16 x the unit-norm embedding
 
-_EPI_F32, _EPI_BF16, _EPI_BIAS_GELU, _EPI_GELU_GRAD = 0, 1, 2, 3
+_EPI_F32, _EPI_BF16, _EPI_BIAS_GELU, _EPI_GELU_GRAD, _EPI_F32_ADD = 0, 1, 2, 3, 4
 
 
 def _gemm(a_t, b_t, epi, M, N, K, A, lda, B, ldb, C, ldc, C2=None, bias=None, aux=None,
@@ -190,9 +190,9 @@ class Embedder:
             cin = self.cin[l]
             prev = bufs.Y[l - 1] if l > 0 else bufs.X0
             dZ = bufs.dZ[l]
-            dWT = torch.empty((5 * cin, D), dtype=torch.float32, device=self.device)
-            # dW^T = im2col(prev)^T . dZ over the P rows
-            _gemm(1, 1, _EPI_F32, 5 * cin, D, P, prev.data_ptr(), cin, _base(dZ), D,
+            dWT = torch.zeros((5 * cin, D), dtype=torch.float32, device=self.device)
+            # dW^T = im2col(prev)^T . dZ over the P rows (split over positions)
+            _gemm(1, 1, _EPI_F32_ADD, 5 * cin, D, P, prev.data_ptr(), cin, _base(dZ), D,
                   dWT.data_ptr(), D)
             db = torch.zeros(D, dtype=torch.float32, device=self.device)
             check(L.sseqs_bias_grad(_base(dZ), P, D, ptr(db), stream_ptr()), "bias_grad")
@@ -255,6 +255,11 @@ class PairSet:
     y: torch.Tensor          # float32 [B]: SW(q, t) / SW(q, q)
     n_queries: int
     per_query: int
+    delim: torch.Tensor      # int32 '@' positions (segment g = sequence g)
+    query_enc: list          # residue classes of every query (device)
+    self_score: torch.Tensor  # float32 [n_queries]
+    qbuf: torch.Tensor = None    # uint8 [n_queries, 2048]: query classes, one row each
+    qlen: torch.Tensor = None    # int32 [n_queries]
 
 
 def training_pairs(n_queries: int, per_query: int, seed: int = 0, ident=(0.15, 1.0),
@@ -320,58 +325,98 @@ def training_pairs(n_queries: int, per_query: int, seed: int = 0, ident=(0.15, 1
             scores[torch.tensor(grp, device=dev)] = out[:, :stride]
     self_s = scores[:, 0:1].clamp(min=1).to(torch.float32)
     y = (scores[:, 1:].to(torch.float32) / self_s).clamp_(0, 1).flatten()
+    qbuf = torch.zeros((n_queries, batched.MAX_QUERY), dtype=torch.uint8, device=dev)
+    for i, e in enumerate(encs):
+        qbuf[i, :e.numel()] = e
+    qlen = torch.tensor([e.numel() for e in encs], dtype=torch.int32, device=dev)
     return PairSet(ascii, offsets, lengths.to(torch.int32), qa.to(torch.int32),
-                   tb.to(torch.int32), y, n_queries, per_query)
+                   tb.to(torch.int32), y, n_queries, per_query, delim, encs,
+                   self_s.flatten(), qbuf, qlen)
+
+
+def _cross_scores(pairs: PairSet, qids, tseq, gap_open=11, gap_extend=1) -> torch.Tensor:
+    """Exact affine SW of every query in ``qids`` (all of one stripe width)
+    against every sequence in ``tseq`` (segment indices of the pair
+    buffer), divided by the query's self-score: float32 [len(qids),
+    len(tseq)].  One batched launch."""
+    from . import batched
+    dev = pairs.ascii.device
+    tg = torch.as_tensor(tseq, dtype=torch.int32, device=dev)
+    q = torch.as_tensor(qids, dtype=torch.int64, device=dev)
+    tpt = tune.tpt_of(int(pairs.query_enc[qids[0]].numel()))
+    sc = batched.sw_scan_queries(pairs.qbuf[q], pairs.qlen[q], tpt, pairs.ascii, pairs.delim,
+                                 affine=True, good_idx=tg, skip=0, gap_a=gap_open,
+                                 gap_b=gap_extend)
+    return (sc[:, :tg.numel()].to(torch.float32) / pairs.self_score[q][:, None]).clamp_(0, 1)
 
 
 def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
           targets_per_query: int = 32, epochs: int = 1, lr: float = 2e-3,
           lr_end: float = 1e-4, seed: int = 0, log=None) -> dict:
-    """Adam on the squared error between embedding cosines and the pairs'
-    normalised SW scores.  Each step takes ``queries_per_step`` queries and
-    ``targets_per_query`` of each one's targets."""
+    """Adam on the squared error between embedding cosines and normalised
+    SW scores.  A step takes ``queries_per_step`` queries with
+    ``targets_per_query`` of each one's targets, and labels EVERY (query,
+    target) pair of the step -- the targets of the other queries serve as
+    negatives -- with the exact affine SW score of the pair divided by the
+    query's self-score, computed for the step by the score kernels."""
     dev = model.device
     rng = np.random.default_rng(seed)
     nq, pq = pairs.n_queries, pairs.per_query
     tq = min(targets_per_query, pq)
-    slices = [(q, t0) for q in range(nq) for t0 in range(0, pq - tq + 1, tq)]
-    total = epochs * (len(slices) // queries_per_step)
-    losses, step = [], 0
+    # a step's queries share one stripe width, so that one launch scores
+    # all its (query, target) pairs
+    qtpt = [tune.tpt_of(int(e.numel())) for e in pairs.query_enc]
+    by_tpt: dict = {}
+    for q in range(nq):
+        for t0 in range(0, pq - tq + 1, tq):
+            by_tpt.setdefault(qtpt[q], []).append((q, t0))
+
+    def plan():
+        steps = []
+        for sl in by_tpt.values():
+            perm = rng.permutation(len(sl))
+            for s0 in range(0, len(sl), queries_per_step):
+                steps.append([sl[i] for i in perm[s0:s0 + queries_per_step]])
+        return [steps[i] for i in rng.permutation(len(steps))]
+
+    total = epochs * len(plan())
+    losses, step, labelled = [], 0, 0
     loss_acc = torch.zeros(1, dtype=torch.float32, device=dev)
     stride = 1 + pq
     for ep in range(epochs):
-        order = rng.permutation(len(slices))
-        for s0 in range(0, len(order) - queries_per_step + 1, queries_per_step):
-            pick = [slices[i] for i in order[s0:s0 + queries_per_step]]
-            seq = []
-            ia, ib, yy = [], [], []
-            for j, (q, t0) in enumerate(pick):
-                base = len(seq)
-                seq.append(q * stride)
-                seq.extend(range(q * stride + 1 + t0, q * stride + 1 + t0 + tq))
-                ia.extend([base] * tq)
-                ib.extend(range(base + 1, base + 1 + tq))
-                yy.append((q * pq + t0, tq))
+        for pick in plan():
+            qids = [q for q, _ in pick]
+            tseq = [q * stride + 1 + t0 + k for q, t0 in pick for k in range(tq)]
+            seq = [q * stride for q in qids] + tseq
             sidx = torch.tensor(seq, dtype=torch.int64, device=dev)
             lay = make_layout(pairs.ascii, pairs.offsets[sidx], pairs.lengths[sidx])
             emb = model.forward(lay, train=True)
-            y = torch.cat([pairs.y[a:a + n] for a, n in yy])
-            ia_t = torch.tensor(ia, dtype=torch.int32, device=dev)
-            ib_t = torch.tensor(ib, dtype=torch.int32, device=dev)
+            y = _cross_scores(pairs, qids, tseq).flatten().contiguous()
+            nqs, nt = len(qids), len(tseq)
+            ia_t = torch.arange(nqs, dtype=torch.int32, device=dev).repeat_interleave(nt)
+            ib_t = (nqs + torch.arange(nt, dtype=torch.int32, device=dev)).repeat(nqs)
+            # half the weight on each query's own targets (homologs and
+            # unrelated), half on the other queries' targets (negatives)
+            owner = torch.arange(nt, device=dev) // tq
+            own = (owner[None, :] == torch.arange(nqs, device=dev)[:, None]).flatten()
+            w = torch.where(own, 0.5 / (nqs * tq), 0.5 / (nqs * max(nt - tq, 1))).to(
+                torch.float32).contiguous()
             dE = torch.zeros_like(emb)
             loss_acc.zero_()
-            check(lib().sseqs_pair_loss(ptr(emb), D, ptr(ia_t), ptr(ib_t), ptr(y), ia_t.numel(),
-                                        ptr(dE), ptr(loss_acc), None, stream_ptr()), "pair_loss")
+            check(lib().sseqs_pair_loss(ptr(emb), D, ptr(ia_t), ptr(ib_t), ptr(y), ptr(w),
+                                        ia_t.numel(), ptr(dE), ptr(loss_acc), None, stream_ptr()),
+                  "pair_loss")
             grads = model.backward(dE)
             frac = step / max(total - 1, 1)
             cur = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * frac))
             model.apply(grads, cur)
+            labelled += ia_t.numel()
             if step % 50 == 0 or step == total - 1:
                 losses.append((step, float(loss_acc.item())))
                 if log:
                     log(f"step {step}/{total} loss {losses[-1][1]:.5f} lr {cur:.2e}")
             step += 1
-    return {"steps": step, "losses": losses}
+    return {"steps": step, "losses": losses, "labelled_pairs": labelled}
 
 
 # ----------------------------------------------------------------- search
@@ -417,7 +462,9 @@ class LearnedIndex:
         L = lib()
         # threshold: the k-th largest score over an evenly spaced sample
         S = min(sample, self.n)
-        rows = torch.linspace(0, self.n - 1, S, device=dev).round().to(torch.int64)
+        # evenly spaced rows in integer arithmetic (float32 cannot hold
+        # every row index of a 20M-row index)
+        rows = torch.arange(S, dtype=torch.int64, device=dev) * (self.n - 1) // max(S - 1, 1)
         samp = self.codes[rows].contiguous()
         dense = torch.empty((nq, S), dtype=torch.float32, device=dev)
         check(L.sseqs_score_dense(ptr(qcodes), nq, ptr(samp), S, ptr(dense), stream_ptr()),
@@ -514,3 +561,22 @@ class LearnedIndex:
         codes = self.query_codes(queries)
         cands, _ = self.candidates(codes, n_cand, **kw)
         return self.rescore(queries, cands, top=top)
+
+
+def hit_strings(db, rows, width: int = 500) -> list:
+    """First ``width`` residues of each hit (rows of ``rescore``), as the
+    exhaustive search reports them (sseqs/msa.py:367-369)."""
+    msa = importlib.import_module("sseqs_b200.msa")
+    out = [None] * len(rows)
+    by_batch: dict = {}
+    for i, r in enumerate(rows):
+        by_batch.setdefault(r[1], []).append(i)
+    for bi, idx in by_batch.items():
+        b = db.batches[bi]
+        # the segment index is used as the exhaustive search uses it
+        g = torch.tensor([rows[i][2] for i in idx], dtype=torch.int32, device=db.device)
+        hb, hl = msa._gather_hits(b, g, len(idx))
+        hb, hl = to_host(hb), to_host(hl)
+        for j, i in enumerate(idx):
+            out[i] = hb[j, :hl[j]].tobytes().decode("latin-1")
+    return out
