@@ -291,7 +291,7 @@ def serving_leg(db, n_requests, rate, seed=4):
             "lengths": "U(50, 1000), seed %d" % seed}
 
 
-def learned_leg(db, exact_rows, n_pairs, n_queries, seed=5):
+def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
     """Learned prefilter: train the conv embedder on ``n_pairs`` seeded
     (query, target) pairs labelled by this package's exact SW, embed every
     database segment into FP8 codes, then per query take 32768 candidates by
@@ -308,7 +308,7 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, seed=5):
     torch.cuda.synchronize()
     t1 = time.time()
     model = learned.Embedder(seed=seed)
-    hist = learned.train(model, pairs, epochs=1, seed=seed)
+    hist = learned.train(model, pairs, epochs=epochs, seed=seed)
     torch.cuda.synchronize()
     t2 = time.time()
     index = learned.LearnedIndex(model, db)
@@ -346,7 +346,8 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, seed=5):
             "recall_of_exact_top1000": round(float(np.mean(rec)), 4) if rec else None,
             "recall_min": round(float(np.min(rec)), 4) if rec else None,
             "recall_queries": len(rec), "candidates_per_query": 32768,
-            "train_pairs": int(pairs.y.numel()), "train_steps": hist["steps"],
+            "train_pairs": int(pairs.y.numel()), "train_epochs": epochs,
+            "train_steps": hist["steps"], "train_labelled_pairs": hist["labelled_pairs"],
             "train_loss_first_last": [hist["losses"][0][1], hist["losses"][-1][1]],
             "params": model.n_params, "seconds_pairs": round(t1 - t0, 1),
             "seconds_train": round(t2 - t1, 1), "seconds_index": round(t3 - t2, 1),
@@ -558,7 +559,8 @@ def bench_b200(args):
     if world == 1 and args.serve_requests > 0:
         out["serving"] = serving_leg(db, args.serve_requests, args.serve_rate)
     if world == 1 and args.learned_pairs > 0:
-        out["learned"] = learned_leg(db, exact_rows, args.learned_pairs, args.learned_queries)
+        out["learned"] = learned_leg(db, exact_rows, args.learned_pairs, args.learned_queries,
+                                     epochs=args.learned_epochs)
         out["learned"]["speedup_vs_exact_step"] = round(
             out["learned"]["queries_per_s"] / out["queries_per_s"], 2)
     if world == 1 and not args.no_cpu_baseline:
@@ -633,6 +635,8 @@ def main():
                     help="training pairs of the learned-prefilter leg; 0 skips it")
     ap.add_argument("--learned-queries", type=int, default=64,
                     help="queries timed in the learned-prefilter leg")
+    ap.add_argument("--learned-epochs", type=int, default=2,
+                    help="training epochs over the learned leg's pairs")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

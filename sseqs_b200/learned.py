@@ -352,13 +352,19 @@ def _cross_scores(pairs: PairSet, qids, tseq, gap_open=11, gap_extend=1) -> torc
 
 def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
           targets_per_query: int = 32, epochs: int = 1, lr: float = 2e-3,
-          lr_end: float = 1e-4, seed: int = 0, log=None) -> dict:
+          lr_end: float = 1e-4, floor: float = 0.5, seed: int = 0, log=None) -> dict:
     """Adam on the squared error between embedding cosines and normalised
     SW scores.  A step takes ``queries_per_step`` queries with
     ``targets_per_query`` of each one's targets, and labels EVERY (query,
     target) pair of the step -- the targets of the other queries serve as
     negatives -- with the exact affine SW score of the pair divided by the
-    query's self-score, computed for the step by the score kernels."""
+    query's self-score, computed for the step by the score kernels.
+
+    The cosine is fitted to ``floor + (1 - floor) * y``: only the order of
+    cosines matters for the search, and asking unrelated pairs for a cosine
+    near 0 drives the pooled features towards cancelling out, after which
+    the normalised embedding of a sequence is mostly noise and some close
+    homologs come out nearly orthogonal."""
     dev = model.device
     rng = np.random.default_rng(seed)
     nq, pq = pairs.n_queries, pairs.per_query
@@ -391,7 +397,7 @@ def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
             sidx = torch.tensor(seq, dtype=torch.int64, device=dev)
             lay = make_layout(pairs.ascii, pairs.offsets[sidx], pairs.lengths[sidx])
             emb = model.forward(lay, train=True)
-            y = _cross_scores(pairs, qids, tseq).flatten().contiguous()
+            y = (floor + (1.0 - floor) * _cross_scores(pairs, qids, tseq)).flatten().contiguous()
             nqs, nt = len(qids), len(tseq)
             ia_t = torch.arange(nqs, dtype=torch.int32, device=dev).repeat_interleave(nt)
             ib_t = (nqs + torch.arange(nt, dtype=torch.int32, device=dev)).repeat(nqs)
