@@ -257,7 +257,7 @@ def batched_leg(db, n_queries, seed=3):
             "cells": cells, "identical_hits": bool(same)}
 
 
-def serving_leg(db, n_requests, rate, seed=4):
+def serving_leg(db, n_requests, rate, seed=4, index=None):
     """Request loop over the resident database (``serve.SearchServer`` with
     the GPU executor): Poisson arrivals at ``rate`` queries/s, query lengths
     U(50, 1000), exact affine scoring of every segment and top-4096 per
@@ -267,8 +267,16 @@ def serving_leg(db, n_requests, rate, seed=4):
     rng = np.random.default_rng(seed)
     queries = [dbtools.random_query(int(L), 9000 + i)
                for i, L in enumerate(rng.integers(50, 1001, n_requests))]
-    ex = serve.GpuExecutor(db, top_k=TOP_K)
-    srv = serve.SearchServer(ex, top_k=TOP_K, max_slots=64)
+    if index is None:
+        ex = serve.GpuExecutor(db, top_k=TOP_K)
+        pipeline = "exact affine SW of every segment, top-4096"
+    else:
+        ex = serve.LearnedExecutor(index, top_k=TOP_K)
+        pipeline = "learned prefilter (FP8 index, 32768 candidates) + exact affine SW, top-4096"
+    import torch
+    free = (lambda: torch.cuda.mem_get_info()[0])
+    srv = serve.SearchServer(ex, top_k=TOP_K, max_slots=64, memory_reserve=2 << 30,
+                             free_memory=free)
     # warm-up outside the measurement (autotune of the widths, first launches)
     from sseqs_b200 import tune
     tune.autotune([len(q) for q in queries], db.batches[0])
@@ -287,7 +295,7 @@ def serving_leg(db, n_requests, rate, seed=4):
     return {"requests": n_requests, "arrival_rate_qps": rate,
             "queries_per_s": round(st.queries_per_s, 3), "p50_ms": round(st.p50_ms, 1),
             "p99_ms": round(st.p99_ms, 1), "mean_ms": round(st.mean_ms, 1),
-            "engine_steps": srv.steps, "pipeline": "exact affine SW of every segment, top-4096",
+            "engine_steps": srv.steps, "pipeline": pipeline,
             "lengths": "U(50, 1000), seed %d" % seed}
 
 
@@ -341,6 +349,7 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
         want = {(r[1], r[2]) for r in ex[:1000]}
         got = {(r[1], r[2]) for r in rows[:1000]}
         rec.append(len(want & got) / max(1, len(want)))
+    learned_leg.index = index
     return {"queries": len(qs), "queries_per_s": round(len(qs) / (ms * 1e-3), 3),
             "ms_per_query": round(ms / len(qs), 2),
             "recall_of_exact_top1000": round(float(np.mean(rec)), 4) if rec else None,
@@ -563,6 +572,11 @@ def bench_b200(args):
                                      epochs=args.learned_epochs)
         out["learned"]["speedup_vs_exact_step"] = round(
             out["learned"]["queries_per_s"] / out["queries_per_s"], 2)
+        if args.serve_requests > 0:
+            out["serving_learned"] = serving_leg(db, 4 * args.serve_requests,
+                                                 args.serve_rate_learned,
+                                                 index=learned_leg.index)
+        learned_leg.index = None
     if world == 1 and not args.no_cpu_baseline:
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
@@ -631,6 +645,8 @@ def main():
                     help="requests of the serving leg; 0 skips it")
     ap.add_argument("--serve-rate", type=float, default=1.5,
                     help="Poisson arrival rate (queries/s) of the serving leg")
+    ap.add_argument("--serve-rate-learned", type=float, default=10.0,
+                    help="Poisson arrival rate (queries/s) of the learned serving leg")
     ap.add_argument("--learned-pairs", type=int, default=1_000_000,
                     help="training pairs of the learned-prefilter leg; 0 skips it")
     ap.add_argument("--learned-queries", type=int, default=64,

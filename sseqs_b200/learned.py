@@ -497,9 +497,12 @@ class LearnedIndex:
             if c <= n_cand:
                 out.append(cand[q, :c])
                 continue
-            keys = cs[q, :c].to(torch.float16)
+            # lists are appended in no fixed order: order them by row first,
+            # so that ties at the cut go to the lower rows, as in every run
+            rows_q, perm = cand[q, :c].sort()
+            keys = cs[q, :c][perm].to(torch.float16)
             p = select.topk_indices(keys, n_cand).long()
-            out.append(cand[q, :c][p])
+            out.append(rows_q[p])
         return out, cnt
 
     def rescore(self, queries, cands, top: int = 4096, gap_open=11, gap_extend=1):

@@ -144,6 +144,44 @@ class GpuExecutor:
         return out
 
 
+class LearnedExecutor:
+    """The learned-prefilter pipeline as one engine step: every request in
+    flight gets its candidates from the FP8 index (all requests of the step
+    in one selection GEMM), exact affine SW of the candidates and its top-k;
+    requests complete in the step that admits them.  The database and its
+    codes stay resident (``learned.LearnedIndex``)."""
+
+    n_batches = 1
+
+    def __init__(self, index, *, top_k: int = 4096, n_cand: int = 32768):
+        self.index, self.top_k, self.n_cand = index, int(top_k), int(n_cand)
+
+    @staticmethod
+    def request_bytes(top_k: int, n_batches: int) -> int:
+        # candidate lists (row + score) at the selection cap, and the hits
+        return 8 * 12 * 32768 + 16 * top_k
+
+    def prepare(self, req: Request) -> None:
+        if not 1 <= len(req.query) <= 2048:
+            raise ValueError(f"query length {len(req.query)} outside 1..2048")
+        req.enc = req.query
+
+    def step(self, bi: int, reqs: list) -> list:
+        queries = [r.enc for r in reqs]
+        codes = self.index.query_codes(queries)
+        cands, _ = self.index.candidates(codes, self.n_cand)
+        rows = self.index.rescore(queries, cands, top=self.top_k)
+        out = []
+        for rr in rows:
+            # (segment, score) with the batch folded into the order; the
+            # server's merge sorts by score, then batch, then segment
+            seg = np.array([r[2] for r in rr], dtype=np.int32)
+            sc = np.array([r[3] for r in rr], dtype=np.int32)
+            bt = np.array([r[1] for r in rr], dtype=np.int32)
+            out.append((seg, sc, bt))
+        return out
+
+
 class SearchServer:
     """Continuous-batching request loop over a resident database."""
 
@@ -236,7 +274,12 @@ class SearchServer:
         now = self.clock()
         finished = []
         for r, part in zip(reqs, res):
-            r.parts.append((bi, part[0], part[1]))
+            if len(part) == 3:            # executor that covers every batch at once
+                for b in np.unique(part[2]):
+                    m = part[2] == b
+                    r.parts.append((int(b), part[0][m], part[1][m]))
+            else:
+                r.parts.append((bi, part[0], part[1]))
             r.seen += 1
         for r in reqs:
             if r.seen >= nb:

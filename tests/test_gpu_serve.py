@@ -48,3 +48,36 @@ def test_served_results_equal_single_query_search():
         got = list(zip((-h.scores.astype(np.int64)).tolist(), h.batch.tolist(),
                        h.segment.tolist()))
         assert got == exp
+
+
+def test_learned_executor_results_do_not_depend_on_the_mix():
+    from sseqs_b200 import dbtools, learned, serve
+    from sseqs_b200.database import Database
+    q0 = dbtools.random_query(200, 17)
+    syn = dbtools.synthetic_db([q0], 3000, 0.02, (0.5, 0.95), seed=17, device="cpu",
+                               chunk_bytes=100_000)
+    db = Database(syn.chunks, bs=100_000)
+    model = learned.Embedder(seed=4)
+    learned.train(model, learned.training_pairs(16, 32, seed=4), queries_per_step=8,
+                  targets_per_query=16)
+    index = learned.LearnedIndex(model, db, chunk=1000)
+    rng = np.random.default_rng(3)
+    queries = [q0] + [dbtools.random_query(int(L), 500 + i)
+                      for i, L in enumerate(rng.integers(30, 600, 5))]
+    alone = []
+    for q in queries:
+        srv = serve.SearchServer(serve.LearnedExecutor(index, top_k=40, n_cand=200), top_k=40)
+        r = srv.submit(q)
+        while srv.step():
+            pass
+        alone.append(r.result)
+    srv = serve.SearchServer(serve.LearnedExecutor(index, top_k=40, n_cand=200), top_k=40)
+    reqs = [srv.submit(q) for q in queries[:2]]
+    srv.step()
+    reqs += [srv.submit(q) for q in queries[2:]]
+    while srv.step():
+        pass
+    for a, r in zip(alone, reqs):
+        assert np.array_equal(a.scores, r.result.scores)
+        assert np.array_equal(a.batch, r.result.batch)
+        assert np.array_equal(a.segment, r.result.segment)
