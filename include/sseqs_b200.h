@@ -256,14 +256,17 @@ int sseqs_sw_variant_words(int affine, int tpt, int wide);
  * 2: C2 = acc + bias (bf16 pre-activation), C = GELU(C2) (bf16, tanh form);
  * 3: C = acc * GELU'(aux) (bf16, aux bf16 with C's stride); 4: C (fp32,
  * zeroed by the caller) += acc with K split over CTAs (for small M x N and
- * long K, as in weight gradients).  row_mask
+ * long K, as in weight gradients); 5: as 2 with res (bf16, C's stride) added
+ * to C (a residual connection); 6: C2 = acc + res, C = C2 * GELU'(aux) (the
+ * gradient through a residual connection).  Epilogues 5 and 6 need
+ * (a_t, b_t) = (0, 0).  row_mask
  * (nullable, uint8 per row of C): rows with 0 are written as 0 (epilogues
  * 1-3).  A, B 16-byte aligned, lda, ldb multiples of 8; a_t needs M % 8 ==
  * 0, b_t N % 8 == 0.  Tensor cores (mma.sync bf16, fp32 accumulation). */
 int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_t K,
                     const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
                     int64_t ldc, void* C2, const float* bias, const void* aux,
-                    const uint8_t* row_mask, cudaStream_t stream);
+                    const uint8_t* row_mask, const void* res, cudaStream_t stream);
 
 /* cls[row0[s] + i] = class of ascii[off[s] + i] for i < len[s] (other rows
  * untouched). */
@@ -287,12 +290,12 @@ int sseqs_pool_normalize(const void* Y, int D, const int64_t* start, const int32
 int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const int32_t* ib,
                     const float* y, const float* weight, int64_t B, float* dE, float* loss,
                     float* pred, cudaStream_t stream);
-/* Gradient of pool_normalize back to the last layer's pre-activation Z:
- * dZ[row] = (dE - emb <emb, dE>) * inv_norm / len * GELU'(Z[row]) for the
- * rows of every sequence (other rows untouched). */
+/* Gradient of pool_normalize back to the last layer: for the rows of every
+ * sequence (other rows untouched) dY = (dE - emb <emb, dE>) * inv_norm /
+ * len, stored in G when G is non-null, and dZ = dY * GELU'(Z). */
 int sseqs_pool_backward(const float* emb, const float* dE, const float* inv_norm,
                         const int64_t* start, const int32_t* len, int n_seqs, int D,
-                        const void* Z, void* dZ, cudaStream_t stream);
+                        const void* Z, void* dZ, void* G, cudaStream_t stream);
 /* db[c] += sum over the P rows of dZ[p][c]. */
 int sseqs_bias_grad(const void* dZ, int64_t P, int D, float* db, cudaStream_t stream);
 /* Adam step of a conv weight W[Cout][5][Cin] (fp32 w, m, v) from dWT

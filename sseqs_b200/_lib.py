@@ -52,13 +52,13 @@ _SIGNATURES = {
     "sseqs_int16x2_peak": (_I, [_P, ctypes.POINTER(_D), _P]),
     "sseqs_sw_set_variant": (_I, [_I, _I, _I]),
     "sseqs_gemm_bf16": (_I, [_I, _I, _I, _I64, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P,
-                             _P, _P, _P]),
+                             _P, _P, _P, _P]),
     "sseqs_embed_layout": (_I, [_P, _P, _P, _P, _I, _P, _P]),
     "sseqs_embed_lookup": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_embed_grad": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_pool_normalize": (_I, [_P, _I, _P, _P, _I, _P, _P, _P, _P]),
     "sseqs_pair_loss": (_I, [_P, _I, _P, _P, _P, _P, _I64, _P, _P, _P, _P]),
-    "sseqs_pool_backward": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P]),
+    "sseqs_pool_backward": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
     "sseqs_bias_grad": (_I, [_P, _I64, _I, _P, _P]),
     "sseqs_adam_conv": (_I, [_P, _P, _P, _P, _I, _I, _F, _F, _F, _F, _I, _P, _P, _P]),
     "sseqs_adam_flat": (_I, [_P, _P, _P, _P, _I64, _F, _F, _F, _F, _I, _P, _P]),

@@ -45,6 +45,8 @@ enum Epi : int {
   EPI_BIAS_GELU = 2,    // Z = acc + bias (bf16, C2), C = gelu(Z) (bf16); masked rows -> 0
   EPI_GELU_GRAD = 3,    // C (bf16) = acc * gelu'(aux);  masked rows -> 0
   EPI_F32_ADD = 4,      // C (fp32) += acc (atomic; split-K partial sums)
+  EPI_BIAS_GELU_RES = 5,  // as 2, then C += res (bf16, C's stride): a residual connection
+  EPI_GELU_GRAD_RES = 6,  // G = acc + res -> C2 (bf16), C = G * gelu'(aux); masked rows -> 0
 };
 
 __device__ __forceinline__ float gelu_f(float z) {
@@ -96,8 +98,9 @@ struct GemmArgs {
   int64_t ldc;
   __nv_bfloat16* C2;          // EPI_BIAS_GELU: pre-activation
   const float* bias;
-  const __nv_bfloat16* aux;   // EPI_GELU_GRAD: pre-activation
+  const __nv_bfloat16* aux;   // EPI_GELU_GRAD(_RES): pre-activation
   const uint8_t* row_mask;    // nullable: 0 = padding row
+  const __nv_bfloat16* res;   // EPI_*_RES: residual term
 };
 
 // A_T: A stored [K][M] (element (m,k) at A[k*lda + m]) instead of [M][K].
@@ -236,17 +239,39 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
           __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
           c[0] = __float2bfloat16_rn(v0);
           if (two) c[1] = __float2bfloat16_rn(v1);
-        } else if (EPI == EPI_BIAS_GELU) {
+        } else if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES) {
           const float z0 = v0 + g.bias[n], z1 = two ? v1 + g.bias[n + 1] : 0.f;
           __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
           __nv_bfloat16* z = g.C2 + m * g.ldc + n;
           const __nv_bfloat16 zb0 = __float2bfloat16_rn(keep ? z0 : 0.f);
           const __nv_bfloat16 zb1 = __float2bfloat16_rn(keep ? z1 : 0.f);
+          float r0 = 0.f, r1 = 0.f;
+          if (EPI == EPI_BIAS_GELU_RES) {
+            const __nv_bfloat16* rs = g.res + m * g.ldc + n;
+            r0 = __bfloat162float(rs[0]);
+            r1 = two ? __bfloat162float(rs[1]) : 0.f;
+          }
           z[0] = zb0;
-          c[0] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb0)) : 0.f);
+          c[0] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb0)) + r0 : 0.f);
           if (two) {
             z[1] = zb1;
-            c[1] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb1)) : 0.f);
+            c[1] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb1)) + r1 : 0.f);
+          }
+        } else if (EPI == EPI_GELU_GRAD_RES) {
+          const __nv_bfloat16* ax = g.aux + m * g.ldc + n;
+          const __nv_bfloat16* rs = g.res + m * g.ldc + n;
+          __nv_bfloat16* c = reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + n;
+          __nv_bfloat16* gg = g.C2 + m * g.ldc + n;
+          const __nv_bfloat16 g0 = __float2bfloat16_rn(keep ? v0 + __bfloat162float(rs[0]) : 0.f);
+          gg[0] = g0;
+          c[0] = __float2bfloat16_rn(keep ? __bfloat162float(g0) *
+                                                gelu_grad(__bfloat162float(ax[0])) : 0.f);
+          if (two) {
+            const __nv_bfloat16 g1 =
+                __float2bfloat16_rn(keep ? v1 + __bfloat162float(rs[1]) : 0.f);
+            gg[1] = g1;
+            c[1] = __float2bfloat16_rn(keep ? __bfloat162float(g1) *
+                                                  gelu_grad(__bfloat162float(ax[1])) : 0.f);
           }
         } else {   // EPI_GELU_GRAD
           const __nv_bfloat16* ax = g.aux + m * g.ldc + n;
@@ -261,6 +286,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
 
 template <bool A_T, bool B_T, int EPI>
 int launch_gemm(const GemmArgs& g, cudaStream_t stream, int splits = 1) {
+  static_assert(EPI >= 0 && EPI <= 6, "epilogue");
   constexpr int A_TILE = A_T ? BK * LDR : BM * LDK;
   constexpr int B_TILE = B_T ? BK * LDR : BN * LDK;
   constexpr size_t smem = sizeof(__nv_bfloat16) * STAGES * (A_TILE + B_TILE);
@@ -361,10 +387,12 @@ __global__ void pair_loss_kernel(const float* emb, int D, const int32_t* ia, con
 
 // Gradient of the pooled, normalised embedding back to the last layer's
 // pre-activation: dpooled = (dE - e <e, dE>) * inv_norm; each real row of
-// sequence s gets dpooled / len, times gelu'(Z).
+// sequence s gets dY = dpooled / len (stored in G when given), and
+// dZ = dY * gelu'(Z).
 __global__ void pool_backward_kernel(const float* emb, const float* dE, const float* inv_norm,
                                      const int64_t* start, const int32_t* len,
-                                     const __nv_bfloat16* Z, __nv_bfloat16* dZ) {
+                                     const __nv_bfloat16* Z, __nv_bfloat16* dZ,
+                                     __nv_bfloat16* G) {
   const int s = blockIdx.x, c = threadIdx.x, D = blockDim.x;
   const float e = emb[(int64_t)s * D + c], g = dE[(int64_t)s * D + c];
   __shared__ float red[32];
@@ -381,9 +409,11 @@ __global__ void pool_backward_kernel(const float* emb, const float* dE, const fl
   const int n = len[s];
   const float dp = (g - e * red[0]) * inv_norm[s] / (float)max(n, 1);
   const int64_t base = start[s] * D + c;
+  const __nv_bfloat16 gb = __float2bfloat16_rn(dp);
   for (int p = 0; p < n; ++p) {
     const int64_t i = base + (int64_t)p * D;
     dZ[i] = __float2bfloat16_rn(dp * gelu_grad(__bfloat162float(Z[i])));
+    if (G) G[i] = gb;
   }
 }
 
@@ -688,7 +718,7 @@ using namespace sseqs::emb;
 extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_t K,
                                const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
                                int64_t ldc, void* C2, const float* bias, const void* aux,
-                               const uint8_t* row_mask, cudaStream_t stream) {
+                               const uint8_t* row_mask, const void* res, cudaStream_t stream) {
   if (M < 0 || N < 0 || K < 0 || (K % BK) != 0) return SSEQS_ERR_ARG;
   if (M == 0 || N == 0) return SSEQS_OK;
   if (!A || !B || !C) return SSEQS_ERR_ARG;
@@ -698,12 +728,15 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
   if (a_t && (M % 8) != 0) return SSEQS_ERR_ARG;
   if (b_t && (N % 8) != 0) return SSEQS_ERR_ARG;
   if (epilogue == EPI_BIAS_GELU && (!bias || !C2)) return SSEQS_ERR_ARG;
-  if (epilogue == EPI_GELU_GRAD && !aux) return SSEQS_ERR_ARG;
-  if (epilogue < 0 || epilogue > 4) return SSEQS_ERR_ARG;
+  if ((epilogue == EPI_GELU_GRAD || epilogue == EPI_GELU_GRAD_RES) && !aux) return SSEQS_ERR_ARG;
+  if ((epilogue == EPI_BIAS_GELU_RES && (!bias || !C2 || !res)) ||
+      (epilogue == EPI_GELU_GRAD_RES && (!C2 || !res)))
+    return SSEQS_ERR_ARG;
+  if (epilogue < 0 || epilogue > 6) return SSEQS_ERR_ARG;
   GemmArgs g{M, N, K, static_cast<const __nv_bfloat16*>(A), lda,
              static_cast<const __nv_bfloat16*>(B), ldb, C, ldc,
              static_cast<__nv_bfloat16*>(C2), bias, static_cast<const __nv_bfloat16*>(aux),
-             row_mask};
+             row_mask, static_cast<const __nv_bfloat16*>(res)};
   if (epilogue == EPI_F32_ADD) {
     // split K so that the grid covers every SM twice (C holds the sum of
     // the partial products; the caller zeroes it)
@@ -712,6 +745,11 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
     const int64_t want = (2 * (int64_t)device_sm_count() + tiles - 1) / tiles;
     const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(want, K / BK));
     return launch_gemm<true, true, EPI_F32_ADD>(g, stream, splits);
+  }
+  if (epilogue == EPI_BIAS_GELU_RES || epilogue == EPI_GELU_GRAD_RES) {
+    if (a_t || b_t) return SSEQS_ERR_UNSUPPORTED;
+    return epilogue == EPI_BIAS_GELU_RES ? launch_gemm<false, false, EPI_BIAS_GELU_RES>(g, stream)
+                                         : launch_gemm<false, false, EPI_GELU_GRAD_RES>(g, stream);
   }
   const int key = (a_t ? 8 : 0) | (b_t ? 4 : 0) | (epilogue & 3);
   switch (key) {
@@ -770,13 +808,14 @@ extern "C" int sseqs_pair_loss(const float* emb, int D, const int32_t* ia, const
 
 extern "C" int sseqs_pool_backward(const float* emb, const float* dE, const float* inv_norm,
                                    const int64_t* start, const int32_t* len, int n_seqs, int D,
-                                   const void* Z, void* dZ, cudaStream_t stream) {
+                                   const void* Z, void* dZ, void* G, cudaStream_t stream) {
   if (n_seqs < 0 || D < 32 || D > 1024 || (D % 32) != 0) return SSEQS_ERR_ARG;
   if (n_seqs == 0) return SSEQS_OK;
   if (!emb || !dE || !inv_norm || !start || !len || !Z || !dZ) return SSEQS_ERR_ARG;
   { pool_backward_kernel<<<n_seqs, D, 0, stream>>>(emb, dE, inv_norm, start, len,
                                                    static_cast<const __nv_bfloat16*>(Z),
-                                                   static_cast<__nv_bfloat16*>(dZ));
+                                                   static_cast<__nv_bfloat16*>(dZ),
+                                                   static_cast<__nv_bfloat16*>(G));
     count_launches(1); }
   return status_of(cudaGetLastError());
 }

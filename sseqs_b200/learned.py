@@ -41,13 +41,14 @@ NCLS = 21
 MAX_LEN = 2048     # residues of a sequence the embedder reads
 CODE_SCALE = 16.0  # FP8 codes hold 16 x the unit-norm embedding
 
-_EPI_F32, _EPI_BF16, _EPI_BIAS_GELU, _EPI_GELU_GRAD, _EPI_F32_ADD = 0, 1, 2, 3, 4
+(_EPI_F32, _EPI_BF16, _EPI_BIAS_GELU, _EPI_GELU_GRAD, _EPI_F32_ADD, _EPI_BIAS_GELU_RES,
+ _EPI_GELU_GRAD_RES) = range(7)
 
 
 def _gemm(a_t, b_t, epi, M, N, K, A, lda, B, ldb, C, ldc, C2=None, bias=None, aux=None,
-          mask=None):
+          mask=None, res=None):
     check(lib().sseqs_gemm_bf16(a_t, b_t, epi, M, N, K, A, lda, B, ldb, C, ldc, C2,
-                                ptr(bias), aux, ptr(mask), stream_ptr()), "gemm_bf16")
+                                ptr(bias), aux, ptr(mask), res, stream_ptr()), "gemm_bf16")
 
 
 @dataclass
@@ -93,6 +94,7 @@ class _Buffers:
         self.Y = [z(D) for _ in range(4)]
         self.Z = [z(D) for _ in range(4)] if train else [z(D)]
         self.dZ = [z(D) for _ in range(4)] if train else None
+        self.G = [z(D) for _ in range(4)] if train else None
         self.dX0 = z(E) if train else None
 
 
@@ -102,11 +104,17 @@ def _base(buf: torch.Tensor) -> int:
 
 
 class Embedder:
-    """The 1D-conv embedder with its Adam state (all parameters on device)."""
+    """The 1D-conv embedder with its Adam state (all parameters on device).
 
-    def __init__(self, seed: int = 0, device="cuda"):
+    With ``residual`` (the default) layers 2-4 add their input to their
+    output (Y_l = GELU(Z_l) + Y_{l-1}), so the pooled embedding keeps the
+    first layer's short-window features, which substitutions disturb far
+    less than the deeper layers' ~17-residue ones."""
+
+    def __init__(self, seed: int = 0, device="cuda", residual: bool = True):
         dev = torch.device(device)
         self.device = dev
+        self.residual = residual
         g = torch.Generator(device="cpu")
         g.manual_seed(seed)
         self.cin = [E, D, D, D]
@@ -160,9 +168,10 @@ class Embedder:
             Y = bufs.Y[l]
             Z = bufs.Z[l] if train else bufs.Z[0]
             # im2col(prev) row p starts at layout row p-2 = buffer row p
-            _gemm(0, 0, _EPI_BIAS_GELU, P, D, 5 * cprev, prev.data_ptr(), cprev,
-                  self.Wb[l].data_ptr(), 5 * cprev, _base(Y), D, _base(Z), self.b[l], None,
-                  lay.mask)
+            res = l > 0 and self.residual
+            _gemm(0, 0, _EPI_BIAS_GELU_RES if res else _EPI_BIAS_GELU, P, D, 5 * cprev,
+                  prev.data_ptr(), cprev, self.Wb[l].data_ptr(), 5 * cprev, _base(Y), D,
+                  _base(Z), self.b[l], None, lay.mask, _base(prev) if res else None)
             prev, cprev = Y, D
         S = lay.n
         pooled = torch.empty((S, D), dtype=torch.float32, device=self.device)
@@ -182,9 +191,11 @@ class Embedder:
         lay, emb, inv = self._cache
         bufs, P, L = self._bufs, lay.P, lib()
         bufs.dZ[3][2:2 + P].zero_()
+        bufs.G[3][2:2 + P].zero_()
         check(L.sseqs_pool_backward(ptr(emb), ptr(dE), ptr(inv), ptr(lay.start),
                                     ptr(lay.length), lay.n, D, _base(bufs.Z[3]),
-                                    _base(bufs.dZ[3]), stream_ptr()), "pool_backward")
+                                    _base(bufs.dZ[3]), _base(bufs.G[3]), stream_ptr()),
+              "pool_backward")
         grads = {"W": [None] * 4, "b": [None] * 4}
         for l in range(3, -1, -1):
             cin = self.cin[l]
@@ -198,7 +209,13 @@ class Embedder:
             check(L.sseqs_bias_grad(_base(dZ), P, D, ptr(db), stream_ptr()), "bias_grad")
             grads["W"][l], grads["b"][l] = dWT, db
             # data gradient through the transposed (flipped) kernel
-            if l > 0:
+            if l > 0 and self.residual:
+                # G_{l-1} = conv_back(dZ_l) + G_l, dZ_{l-1} = G_{l-1} * GELU'(Z_{l-1})
+                _gemm(0, 0, _EPI_GELU_GRAD_RES, P, cin, 5 * D, dZ.data_ptr(), D,
+                      self.Wf[l].data_ptr(), 5 * D, _base(bufs.dZ[l - 1]), cin,
+                      _base(bufs.G[l - 1]), None, _base(bufs.Z[l - 1]), lay.mask,
+                      _base(bufs.G[l]))
+            elif l > 0:
                 _gemm(0, 0, _EPI_GELU_GRAD, P, cin, 5 * D, dZ.data_ptr(), D,
                       self.Wf[l].data_ptr(), 5 * D, _base(bufs.dZ[l - 1]), cin, None, None,
                       _base(bufs.Z[l - 1]), lay.mask)

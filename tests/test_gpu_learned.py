@@ -77,8 +77,9 @@ def _ref_embed(model, seqs):
         x = E[cls].T[None]                                  # [1, 32, L]
         for l in range(4):
             w = model.Wb[l].float().reshape(256, 5, -1).permute(0, 2, 1)   # [co, ci, 5]
-            x = torch.nn.functional.conv1d(x, w, model.b[l], padding=2)
-            x = torch.nn.functional.gelu(x, approximate="tanh")
+            y = torch.nn.functional.conv1d(x, w, model.b[l], padding=2)
+            y = torch.nn.functional.gelu(y, approximate="tanh")
+            x = y + x if (l > 0 and model.residual) else y
         p = x[0].mean(1)
         outs.append(p / p.norm())
     return torch.stack(outs)
@@ -93,9 +94,10 @@ def _layout_of(seqs):
     return learned.make_layout(ascii, offs, lens)
 
 
-def test_embedder_forward_matches_fp32_conv():
+@pytest.mark.parametrize("residual", [True, False])
+def test_embedder_forward_matches_fp32_conv(residual):
     from sseqs_b200 import dbtools, learned
-    model = learned.Embedder(seed=3)
+    model = learned.Embedder(seed=3, residual=residual)
     seqs = [dbtools.random_query(int(n), 40 + i) for i, n in enumerate([1, 5, 37, 300, 1000])]
     seqs[3] = seqs[3][:20] + "XBZU" + seqs[3][24:]
     got = model.forward(_layout_of(seqs))
@@ -105,9 +107,10 @@ def test_embedder_forward_matches_fp32_conv():
     assert bool((cos > 0.999).all()), cos
 
 
-def test_embedder_backward_matches_autograd():
+@pytest.mark.parametrize("residual", [True, False])
+def test_embedder_backward_matches_autograd(residual):
     from sseqs_b200 import dbtools, learned
-    model = learned.Embedder(seed=5)
+    model = learned.Embedder(seed=5, residual=residual)
     seqs = [dbtools.random_query(int(n), 60 + i) for i, n in enumerate([50, 120, 80, 200])]
     lay = _layout_of(seqs)
     emb = model.forward(lay, train=True)
@@ -126,8 +129,9 @@ def test_embedder_backward_matches_autograd():
         cls = torch.tensor([AA.index(c) if c in AA else 20 for c in s], device="cuda")
         x = Ep[cls].T[None]
         for l in range(4):
-            x = torch.nn.functional.conv1d(x, Ws[l].permute(0, 2, 1), bs[l], padding=2)
-            x = torch.nn.functional.gelu(x, approximate="tanh")
+            y = torch.nn.functional.conv1d(x, Ws[l].permute(0, 2, 1), bs[l], padding=2)
+            y = torch.nn.functional.gelu(y, approximate="tanh")
+            x = y + x if (l > 0 and model.residual) else y
         p = x[0].mean(1)
         tot = tot + ((p / p.norm()) * r[si]).sum()
     tot.backward()
