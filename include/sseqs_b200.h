@@ -268,6 +268,16 @@ int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_
                     int64_t ldc, void* C2, const float* bias, const void* aux,
                     const uint8_t* row_mask, const void* res, cudaStream_t stream);
 
+/* sseqs_gemm_bf16 runs on the 5th-generation tensor cores (tcgen05.mma,
+ * fp32 accumulators in tensor memory) when a_t = b_t = 0, N = 256, K is a
+ * multiple of 64, ldc a multiple of 8, C/C2/aux/res 16-byte aligned and the
+ * epilogue is 1, 2, 3, 5 or 6; otherwise on mma.sync.  set_tensor_path(0)
+ * forces mma.sync (1 restores the default).  gemm_error reads and clears the
+ * flag a tcgen05 launch sets when one of its bounded waits ran out
+ * (synchronous). */
+int sseqs_gemm_set_tensor_path(int tcgen05);
+int sseqs_gemm_error(int* out);
+
 /* cls[row0[s] + i] = class of ascii[off[s] + i] for i < len[s] (other rows
  * untouched). */
 int sseqs_embed_layout(const uint8_t* ascii, const int64_t* off, const int32_t* len,

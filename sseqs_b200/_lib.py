@@ -53,6 +53,8 @@ _SIGNATURES = {
     "sseqs_sw_set_variant": (_I, [_I, _I, _I]),
     "sseqs_gemm_bf16": (_I, [_I, _I, _I, _I64, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P,
                              _P, _P, _P, _P]),
+    "sseqs_gemm_set_tensor_path": (_I, [_I]),
+    "sseqs_gemm_error": (_I, [ctypes.POINTER(_I)]),
     "sseqs_embed_layout": (_I, [_P, _P, _P, _P, _I, _P, _P]),
     "sseqs_embed_lookup": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_embed_grad": (_I, [_P, _I64, _P, _I, _P, _P]),

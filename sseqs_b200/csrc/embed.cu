@@ -29,6 +29,7 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "common.cuh"
 
@@ -299,6 +300,248 @@ int launch_gemm(const GemmArgs& g, cudaStream_t stream, int splits = 1) {
   if (grid.y > 65535u || grid.z > 65535u) return SSEQS_ERR_UNSUPPORTED;
   { fn<<<grid, GEMM_THREADS, smem, stream>>>(g); count_launches(1); }
   return status_of(cudaGetLastError());
+}
+
+// ------------------------------------------------------- tcgen05 GEMM
+// The N = 256 conv GEMMs (forward of layers 2-4, data gradients of layers
+// 1-3) on the 5th-generation tensor cores: C[128 x 256] per CTA accumulates
+// in tensor memory (256 fp32 columns x 128 lanes), fed from shared memory.
+//
+// Shared-memory operands use the K-major, no-swizzle canonical layout of
+// the MMA: 8-row x 16-byte "core matrices" (8 rows x 8 bf16 of K), the
+// core matrices of one 8-row group along K 128 bytes apart (leading byte
+// offset) and consecutive 8-row groups 1024 bytes apart (stride byte
+// offset) for a 64-wide K tile: element (row r, k) of a tile sits at
+// (r/8)*1024 + (k/8)*128 + (r%8)*16 + (k%8)*2.  cp.async writes the tiles
+// (two stages of A 16 KB + B 32 KB, two CTAs per SM, each with 256 of the
+// SM's 512 tensor-memory columns); one thread issues the MMAs of a
+// stage (K 16 each) and commits them to the stage's mbarrier, which the
+// loaders wait on before reusing the stage.  Every wait is bounded: a
+// wait that runs out sets *err and the kernel stops issuing work.  The
+// epilogue reads the accumulators with tcgen05.ld (warp w reads lanes
+// 32(w%4)..+31 = output rows, warps 0-3 columns 0-127 and warps 4-7
+// columns 128-255) and applies the same fused epilogues as the mma.sync
+// kernel.
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 64, TC_STAGES = 2, TC_THREADS = 256;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2, TC_B_BYTES = TC_BN * TC_BK * 2;
+constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
+constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024;
+constexpr unsigned kWaitLimit = 1u << 26;
+
+// Shared-memory matrix descriptor: start, leading (K) and stride (MN)
+// byte offsets in 16-byte units, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;            // version
+  return d;                          // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor, kind::f16: fp32 accumulate, bf16 A and B, both
+// K-major, M = 128, N = 256.
+constexpr uint32_t kIdescBf16 = (1u << 4)            // D format F32
+                              | (1u << 7)            // A format BF16
+                              | (1u << 10)           // B format BF16
+                              | ((uint32_t)(TC_BN >> 3) << 17)
+                              | ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (unsigned i = 0; i < kWaitLimit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int* err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  // align the tile area to 1024 bytes
+  const uint32_t raw = smem_u32(tsm);
+  unsigned char* tiles = tsm + ((1024 - (raw & 1023)) & 1023);
+  __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int abort_s;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * TC_BM;
+  const int64_t ktiles = g.K / TC_BK;
+
+  if (warp == 0) {
+    const uint32_t dst = smem_u32(&tmem_base_s);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(dst), "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < TC_STAGES; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[s])), "r"(1));
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+
+  auto load_stage = [&](int stage, int64_t kt) {
+    unsigned char* a = tiles + stage * TC_STAGE_BYTES;
+    unsigned char* b = a + TC_A_BYTES;
+    const int64_t k0 = kt * TC_BK;
+    // A: 128 rows x 8 chunks of 16 B
+    for (int c = tid; c < TC_BM * 8; c += TC_THREADS) {
+      const int r = c >> 3, kc = c & 7;
+      const int64_t m = m0 + r;
+      const bool ok = m < g.M;
+      cp_async16(a + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16,
+                 g.A + (ok ? m : 0) * g.lda + k0 + kc * 8, ok);
+    }
+    // B: 256 rows x 8 chunks
+    for (int c = tid; c < TC_BN * 8; c += TC_THREADS) {
+      const int r = c >> 3, kc = c & 7;
+      cp_async16(b + (r >> 3) * 1024 + kc * 128 + (r & 7) * 16,
+                 g.B + (int64_t)r * g.ldb + k0 + kc * 8, true);
+    }
+  };
+
+  // prologue: stages 0 .. S-2
+  for (int s = 0; s < TC_STAGES - 1; ++s) {
+    if (s < ktiles) load_stage(s, s);
+    cp_commit();
+  }
+  uint32_t phase[TC_STAGES] = {};
+  bool ok = true;
+  for (int64_t kt = 0; kt < ktiles && ok; ++kt) {
+    const int stage = (int)(kt % TC_STAGES);
+    // refill the stage of tile kt + S - 1 once the MMAs that read it (tile
+    // kt - 1) are done
+    {
+      const int64_t nk = kt + TC_STAGES - 1;
+      const int ns = (int)(nk % TC_STAGES);
+      if (nk < ktiles) {
+        if (kt >= 1) {
+          if (!mbar_wait(smem_u32(&mbar[ns]), phase[ns])) { if (tid == 0) abort_s = 1; }
+          phase[ns] ^= 1;
+        }
+        load_stage(ns, nk);
+      }
+      cp_commit();
+    }
+    cp_wait<TC_STAGES - 1>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (abort_s) { ok = false; break; }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(tiles + stage * TC_STAGE_BYTES);
+      const uint32_t b0 = a0 + TC_A_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < TC_BK / 16; ++ks) {
+        const uint64_t da = umma_desc(a0 + ks * 256, 128, 1024);
+        const uint64_t db = umma_desc(b0 + ks * 256, 128, 1024);
+        const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tmem), "l"(da), "l"(db), "r"(kIdescBf16), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(&mbar[stage])) : "memory");
+    }
+  }
+  cp_wait<0>();
+  // wait for the last tile's MMAs (they complete in order, so this covers all)
+  if (ok && ktiles > 0) {
+    const int ls = (int)((ktiles - 1) % TC_STAGES);
+    // the stage's barrier has completed one phase per tile it held; the
+    // parity of the last one is the number of earlier completions mod 2
+    const uint32_t par = (uint32_t)(((ktiles - 1) / TC_STAGES) & 1);
+    if (!mbar_wait(smem_u32(&mbar[ls]), par)) ok = false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    const int wq = warp & 3;                       // lanes 32*wq .. +31
+    const int64_t m = m0 + wq * 32 + lane;
+    const bool row_ok = m < g.M;
+    const bool keep = row_ok && (g.row_mask ? g.row_mask[m] != 0 : true);
+    const int cbeg = (warp >> 2) * (TC_BN / 2);
+#pragma unroll 1
+    for (int c0 = cbeg; c0 < cbeg + TC_BN / 2; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+          "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+            "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+            "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+            "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!row_ok) continue;
+      // this row's 32 residual / pre-activation values, 16 bytes at a time
+      __align__(16) __nv_bfloat16 rs[32], ax[32];
+      if (EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+        const uint4* src = reinterpret_cast<const uint4*>(g.res + m * g.ldc + c0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(rs)[q] = src[q];
+      }
+      if (EPI == EPI_GELU_GRAD || EPI == EPI_GELU_GRAD_RES) {
+        const uint4* src = reinterpret_cast<const uint4*>(g.aux + m * g.ldc + c0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(ax)[q] = src[q];
+      }
+      __align__(16) __nv_bfloat16 outc[32], outz[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int64_t n = c0 + j;
+        const float acc = __uint_as_float(v[j]);
+        float cval = 0.f, zval = 0.f;
+        if (EPI == EPI_BF16) {
+          cval = keep ? acc : 0.f;
+        } else if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES) {
+          const __nv_bfloat16 zb = __float2bfloat16_rn(keep ? acc + g.bias[n] : 0.f);
+          zval = __bfloat162float(zb);
+          const float r = (EPI == EPI_BIAS_GELU_RES) ? __bfloat162float(rs[j]) : 0.f;
+          cval = keep ? gelu_f(zval) + r : 0.f;
+        } else if (EPI == EPI_GELU_GRAD) {
+          cval = keep ? acc * gelu_grad(__bfloat162float(ax[j])) : 0.f;
+        } else {   // EPI_GELU_GRAD_RES
+          const __nv_bfloat16 gb = __float2bfloat16_rn(keep ? acc + __bfloat162float(rs[j]) : 0.f);
+          zval = __bfloat162float(gb);
+          cval = keep ? zval * gelu_grad(__bfloat162float(ax[j])) : 0.f;
+        }
+        outc[j] = __float2bfloat16_rn(cval);
+        outz[j] = __float2bfloat16_rn(zval);
+      }
+      uint4* dc = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + c0);
+      const uint4* sc = reinterpret_cast<const uint4*>(outc);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dc[q] = sc[q];
+      if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+        uint4* dz = reinterpret_cast<uint4*>(g.C2 + m * g.ldc + c0);
+        const uint4* sz = reinterpret_cast<const uint4*>(outz);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dz[q] = sz[q];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_BN));
 }
 
 // ------------------------------------------------------------ elementwise
@@ -715,6 +958,52 @@ int grid_for(int64_t work, int threads) {
 using namespace sseqs;
 using namespace sseqs::emb;
 
+static __device__ int g_tc_err;
+static bool g_tc_enabled = true;
+
+static int* tc_err_ptr() {
+  static int* p[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!p[dev]) {
+    void* q = nullptr;
+    if (cudaGetSymbolAddress(&q, g_tc_err) != cudaSuccess) return nullptr;
+    p[dev] = static_cast<int*>(q);
+  }
+  return p[dev];
+}
+
+template <int EPI>
+int launch_tc(const GemmArgs& g, cudaStream_t stream) {
+  auto fn = gemm_tc_kernel<EPI>;
+  int* err = tc_err_ptr();
+  if (!err) return SSEQS_ERR_CUDA;
+  if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TC_SMEM) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const int64_t grid = (g.M + TC_BM - 1) / TC_BM;
+  if (grid > INT32_MAX) return SSEQS_ERR_UNSUPPORTED;
+  { fn<<<(unsigned)grid, TC_THREADS, TC_SMEM, stream>>>(g, err); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
+// 1 = use the tcgen05 kernel where it applies (default), 0 = mma.sync only.
+extern "C" int sseqs_gemm_set_tensor_path(int tcgen05) {
+  g_tc_enabled = tcgen05 != 0;
+  return SSEQS_OK;
+}
+
+// Reads and clears the flag a tcgen05 GEMM sets when one of its bounded
+// waits runs out (synchronises the device).
+extern "C" int sseqs_gemm_error(int* out) {
+  int* p = tc_err_ptr();
+  if (!p || !out) return SSEQS_ERR_ARG;
+  int zero = 0;
+  if (cudaMemcpy(out, p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SSEQS_ERR_CUDA;
+  if (cudaMemcpy(p, &zero, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return SSEQS_ERR_CUDA;
+  return SSEQS_OK;
+}
+
 extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_t K,
                                const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
                                int64_t ldc, void* C2, const float* bias, const void* aux,
@@ -745,6 +1034,21 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
     const int64_t want = (2 * (int64_t)device_sm_count() + tiles - 1) / tiles;
     const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(want, K / BK));
     return launch_gemm<true, true, EPI_F32_ADD>(g, stream, splits);
+  }
+  // N = 256, K % 64 == 0, row-major operands: the tcgen05 kernel
+  if (g_tc_enabled && !a_t && !b_t && N == TC_BN && K >= TC_BK && (K % TC_BK) == 0 &&
+      (ldc % 8) == 0 &&
+      (reinterpret_cast<uintptr_t>(C) & 15) == 0 && (!C2 || (reinterpret_cast<uintptr_t>(C2) & 15) == 0) &&
+      (!res || (reinterpret_cast<uintptr_t>(res) & 15) == 0) &&
+      (!aux || (reinterpret_cast<uintptr_t>(aux) & 15) == 0) &&
+      epilogue != EPI_F32 && epilogue != EPI_F32_ADD) {
+    switch (epilogue) {
+      case EPI_BF16: return launch_tc<EPI_BF16>(g, stream);
+      case EPI_BIAS_GELU: return launch_tc<EPI_BIAS_GELU>(g, stream);
+      case EPI_GELU_GRAD: return launch_tc<EPI_GELU_GRAD>(g, stream);
+      case EPI_BIAS_GELU_RES: return launch_tc<EPI_BIAS_GELU_RES>(g, stream);
+      case EPI_GELU_GRAD_RES: return launch_tc<EPI_GELU_GRAD_RES>(g, stream);
+    }
   }
   if (epilogue == EPI_BIAS_GELU_RES || epilogue == EPI_GELU_GRAD_RES) {
     if (a_t || b_t) return SSEQS_ERR_UNSUPPORTED;

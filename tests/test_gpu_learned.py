@@ -52,6 +52,63 @@ def test_gemm_nt_matches_fp32(M, N, K, epi):
     assert err <= tol * max(1.0, exp.abs().max().item()), err
 
 
+def _gemm_error():
+    import ctypes
+    from sseqs_b200 import _lib
+    v = ctypes.c_int(-1)
+    _lib.check(_lib.lib().sseqs_gemm_error(ctypes.byref(v)), "gemm_error")
+    return v.value
+
+
+@pytest.mark.parametrize("M", [1, 131, 5000])
+@pytest.mark.parametrize("epi", [1, 2, 3, 5, 6])
+@pytest.mark.parametrize("K", [64, 1280])
+def test_tcgen05_gemm_matches_mma_sync_and_fp32(M, epi, K):
+    """N = 256 GEMMs take the tcgen05 kernel; the same call on the mma.sync
+    kernel and an fp32 reference must agree (fp32 accumulation of exact
+    bf16 products in both; outputs rounded to bf16)."""
+    from sseqs_b200 import _lib, learned
+    g = torch.Generator(device="cpu")
+    g.manual_seed(M * 7 + epi * 3 + K)
+    N = 256
+    A = _bf(torch.randn(M, K, generator=g)).cuda()
+    B = _bf(torch.randn(N, K, generator=g)).cuda()
+    bias = torch.randn(N, generator=g).cuda()
+    aux = _bf(torch.randn(M, N, generator=g)).cuda()
+    res = _bf(torch.randn(M, N, generator=g)).cuda()
+    mask = (torch.rand(M, generator=g) > 0.2).to(torch.uint8).cuda()
+    outs = []
+    for path in (1, 0):
+        _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(path), "path")
+        C = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda")
+        C2 = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda")
+        learned._gemm(0, 0, epi, M, N, K, A.data_ptr(), K, B.data_ptr(), K, C.data_ptr(), N,
+                      C2.data_ptr(), bias, aux.data_ptr(), mask, res.data_ptr())
+        torch.cuda.synchronize()
+        outs.append((C.float(), C2.float()))
+    _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(1), "path")
+    assert _gemm_error() == 0
+    ref = A.float() @ B.float().T
+    m = mask.bool()[:, None]
+    if epi == 1:
+        exp = torch.where(m, ref, 0)
+    elif epi in (2, 5):
+        z = _bf(ref + bias).float()
+        exp = torch.where(m, torch.nn.functional.gelu(z, approximate="tanh") +
+                          (res.float() if epi == 5 else 0), 0)
+    else:
+        gg = _bf(ref + res.float()).float() if epi == 6 else ref
+        zf = aux.float()
+        t = torch.tanh(0.7978845608 * (zf + 0.044715 * zf ** 3))
+        gp = 0.5 * (1 + t) + 0.5 * zf * (1 - t * t) * 0.7978845608 * (1 + 0.134145 * zf * zf)
+        exp = torch.where(m, gg * gp, 0)
+    scale = max(1.0, exp.abs().max().item())
+    for C, C2 in outs:
+        assert (C - exp).abs().max().item() <= 2e-2 * scale
+    # the two kernels agree up to the bf16 rounding of their outputs
+    assert (outs[0][0] - outs[1][0]).abs().max().item() <= 2e-2 * scale
+
+
 @pytest.mark.parametrize("M,N,K", [(160, 256, 96), (1280, 256, 4096), (40, 24, 32)])
 def test_gemm_tn_matches_fp32(M, N, K):
     from sseqs_b200 import learned
