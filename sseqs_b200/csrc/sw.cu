@@ -163,6 +163,11 @@ int launch_stream(SwArgs a, bool aff, const QueryTable* qt, cudaStream_t stream)
       return SSEQS_ERR_CUDA;
     const int64_t need = (p.n + k.groups_per_block - 1) / k.groups_per_block;
     const int grid = (int)std::max<int64_t>(1, std::min(full, need));
+    // targets per grab: at most 64/TPT (few atomics on long rows of work),
+    // and small enough that every lane group gets about 8 grabs
+    const int64_t groups = (int64_t)grid * k.groups_per_block;
+    p.chunk = (int)std::max<int64_t>(
+        1, std::min<int64_t>(std::max(1, 64 / tpt), p.n / std::max<int64_t>(1, groups * 8)));
     { k.fn<<<dim3(grid, ny), k.threads, k.smem, stream>>>(p, table); count_launches(1); }
     const int st = status_of(cudaGetLastError());
     if (st != SSEQS_OK) return st;

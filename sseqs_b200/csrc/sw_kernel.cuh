@@ -70,6 +70,7 @@ struct SwArgs {
   int32_t* out;
   int p0, p1;             // linear: gap; affine: open, extend
   unsigned int* ticket;   // zeroed launch-wide target counter (fast kernel)
+  int chunk;              // targets per counter grab (fast kernel, >= 1)
 };
 
 // Several queries of the same stripe width in one launch: blockIdx.y picks
@@ -344,10 +345,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
   // ---- target order (group-uniform).  The group leader takes CH targets
   // at a time from the launch-wide counter; the grab for the chunk after
   // the current one is issued when the current one is taken, and its value
-  // is broadcast to the group only when that chunk is reached.
+  // is broadcast to the group only when that chunk is reached.  The host
+  // sizes CH so that every group gets several chunks.
   // The host splits launches so that n < 2^30: target indices and the
   // counter (which overshoots n by at most two grabs per group) fit 32 bits.
-  constexpr int CH = (64 / TPT) > 1 ? 64 / TPT : 1;
+  const int CH = a.chunk;
   const int n = (int)a.n;
   unsigned pre_raw = 0;   // leader only: start of the prefetched chunk
   auto issue_grab = [&]() {
