@@ -36,8 +36,8 @@
 // Targets are streamed: each lane group takes targets from a launch-wide
 // counter (a few at a time, the next grab issued one chunk ahead so its
 // latency is hidden), which keeps every group busy until the last targets
-// whatever their lengths.  A target is read R rows at a time (4 linear, 8
-// affine), the R bytes of the next step prefetched with R/4 + 1 aligned
+// whatever their lengths.  A target is read R rows at a time (4, 8 or 16,
+// see rows_per_fetch), the R bytes of the next step prefetched with R/4 + 1 aligned
 // 32-bit loads; when a target ends (rows past its end are padding rows) the
 // group writes its score, resets its state and moves on while the other
 // groups of the warp keep going.
@@ -52,11 +52,13 @@ namespace sw {
 
 constexpr int kMaxQuery = 2048;
 // Target rows per byte fetch: the per-fetch bookkeeping is shared by this
-// many rows, and a target's last fetch pads with up to R-1 rows.  The affine
-// kernel takes 8 (measured 10% faster than 4 at query length 858); the
-// linear kernel keeps 4, where 8 gained nothing and made the compiler spill.
-template <bool AFF>
-__host__ __device__ constexpr int rows_per_fetch() { return AFF ? 8 : 4; }
+// many rows, and a target's last fetch pads with up to R-1 rows.  Measured
+// (300k targets): affine 8 rows beat 4 by 10% at 27 words per lane, and 16
+// beat 8 by 2-3% at 16 words or fewer but lost 9% at 27 (larger code and
+// register footprint).  Linear 8 rows beat 4 by 3-7% where it fits, but
+// spills under the register caps of many widths, so linear keeps 4.
+template <bool AFF, int NWD>
+__host__ __device__ constexpr int rows_per_fetch() { return AFF ? (NWD <= 16 ? 16 : 8) : 4; }
 
 struct SwArgs {
   const uint8_t* q;       // query residue classes
@@ -307,7 +309,7 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
   // ---- target bytes: R rows at a time from R/4 + 1 aligned 32-bit words.
   // A word is loaded only when it holds a byte of the window being read, so
   // no load leaves the windows' own 4-byte words.
-  constexpr int R = rows_per_fetch<AFF>();
+  constexpr int R = rows_per_fetch<AFF, L::NWD>();
   constexpr int NWORDS = R / 4 + 1;
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
