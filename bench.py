@@ -112,6 +112,11 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- GPU side
+# DRAM traffic of the affine score kernel per target residue, from its ncu
+# capture at 1M sequences (384.4 MB read + 7.4 MB written, 372.7M residues)
+TRAFFIC_BYTES_PER_RESIDUE = (384.404992e6 + 7.380992e6) / 372662216
+
+
 def build_database(queries, db_seqs, seed=0):
     import torch
     from sseqs_b200 import dbtools
@@ -150,7 +155,7 @@ def run_step(M, query, db, timer=None, world=1, rank=0):
 
 
 def prefiltered_leg(M, db, queries, exact_rows, per_query=32768):
-    """configs[1] as specified: FFT prefilter keeping ~per_query candidates
+    """The prefiltered search: the reference's prefilter keeping ~per_query candidates
     per query (top_fft = segments per batch // (per_query / batches)), exact
     linear + affine SW of the candidates, top-4096, traceback.  Reports
     queries/s and recall of the exact search's top-1000 hits."""
@@ -541,7 +546,14 @@ def bench_b200(args):
             "peak": round(alu_peak / 1e9, 1),
             "unit": "Gop/s",
             "frac": round(achieved / alu_peak, 4),
-            "traffic": None,
+            # DRAM bytes of one affine launch (one database batch): the ncu
+            # capture of this kernel on a 1M-sequence batch read 384.4 MB and
+            # wrote 7.4 MB for 372.7M residues, i.e. ~1.05 B per residue,
+            # scaled here to the residues of an average batch of this database
+            "traffic": int(TRAFFIC_BYTES_PER_RESIDUE * res_cells / max(1, len(db.batches))),
+            "traffic_source": "ncu dram__bytes_read+write of the affine launch at 1M sequences "
+                              "(391.8 MB / 372.7M residues), scaled to an average batch",
+            "algorithmic_bytes": int(res_cells / max(1, len(db.batches))),
             "ops_model": "3.5 ALU-pipe DPX int16x2 instructions per 2 cells (affine kernel)",
             "peak_source": "sseqs_dpx_peak measured in this run: ALU-pipe int16x2 DPX issue rate",
             "dual_pipe": {"achieved": round(aff_rate * 5.5 / 2 / 1e9, 1),
