@@ -98,6 +98,19 @@ int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
                   const uint8_t* ascii, const int32_t* delim, int skip,
                   int32_t* out, int gap_a, int gap_b, cudaStream_t stream);
 
+/* Both scores of sseqs_sw_scan in one pass: out_linear[t] is the linear
+ * score (gap, windows as sseqs_sw_scan with skip 0) and out_affine[t] the
+ * affine score (gap_open, gap_extend, windows starting affine_skip (0 or 1)
+ * bytes later) of every target -- identical to the two separate calls
+ * (the exact search of sseqs/msa.py:313-332 with top_sw = 1 makes both).
+ * Gap parameters must lie in the int16 domain, else SSEQS_ERR_UNSUPPORTED
+ * (make the two calls instead).  Queries of up to 512 residues run one
+ * fused kernel; longer ones run the two score kernels in turn. */
+int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len, const int32_t* good_idx,
+                       int32_t g0, int64_t n_targets, const uint8_t* ascii, const int32_t* delim,
+                       int affine_skip, int32_t* out_linear, int32_t* out_affine, int gap,
+                       int gap_open, int gap_extend, cudaStream_t stream);
+
 /* sseqs_sw_scan for several queries of one stripe width against one batch,
  * in one launch per 128 queries (the batched path; the reference runs one
  * query at a time, sseqs/msa.py:235).  Query i has query_lens[i] (device

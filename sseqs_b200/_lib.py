@@ -32,6 +32,8 @@ _SIGNATURES = {
     "sseqs_sw_linear": (_I, [_P, _I, _P, _P, _P, _I64, _P, _I, _P]),
     "sseqs_sw_affine": (_I, [_P, _I, _P, _P, _P, _I64, _P, _I, _I, _P]),
     "sseqs_sw_scan": (_I, [_I, _P, _I, _P, ctypes.c_int32, _I64, _P, _P, _I, _P, _I, _I, _P]),
+    "sseqs_sw_scan_both": (_I, [_P, _I, _P, ctypes.c_int32, _I64, _P, _P, _I, _P, _P, _I, _I, _I,
+                                _P]),
     "sseqs_sw_scan_queries": (_I, [_I, _I, _I, _P, _I64, _P, _P, _I64, ctypes.c_int32, _I64,
                                    _P, _P, _I, _P, _I64, _I, _I, _P, _P]),
     "sseqs_find_delims_workspace_bytes": (_SZ, [_I64]),

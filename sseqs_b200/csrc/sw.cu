@@ -90,8 +90,8 @@ const Tables& tables() {
 
 struct Cache {
   std::mutex mu;
-  int max_blocks[2][2][64][64] = {};  // [variant][affine][TPT-1][device]
-  int variant[2][64] = {};            // chosen variant per [affine][TPT-1]
+  int max_blocks[2][3][64][64] = {};  // [variant][mode][TPT-1][device]
+  int variant[3][64] = {};            // chosen variant per [mode][TPT-1]
 };
 Cache& cache() {
   static Cache c;
@@ -120,7 +120,7 @@ unsigned int* ticket_slot(int dev) {
 // Launches the streaming kernel for one query (qt == nullptr; target
 // counter from the ring) or for the qt->n queries of a table (counters
 // a.ticket[0 .. qt->n), provided by the caller).
-int launch_stream(SwArgs a, bool aff, const QueryTable* qt, cudaStream_t stream) {
+int launch_stream(SwArgs a, int mode, const QueryTable* qt, cudaStream_t stream) {
   const int tpt = (a.Lq + 31) / 32;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
@@ -128,9 +128,9 @@ int launch_stream(SwArgs a, bool aff, const QueryTable* qt, cudaStream_t stream)
   const KernelInfo* kp;
   {
     std::lock_guard<std::mutex> lk(cache().mu);
-    var = cache().variant[aff][tpt - 1];
-    kp = &tables().k[var][aff][tpt - 1];
-    int& mb = cache().max_blocks[var][aff][tpt - 1][dev];
+    var = cache().variant[mode][tpt - 1];
+    kp = &tables().k[var][mode][tpt - 1];
+    int& mb = cache().max_blocks[var][mode][tpt - 1][dev];
     if (mb == 0) {
       if (cudaFuncSetAttribute((const void*)kp->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kp->smem) != cudaSuccess)
@@ -155,6 +155,7 @@ int launch_stream(SwArgs a, bool aff, const QueryTable* qt, cudaStream_t stream)
     SwArgs p = a;
     p.n = std::min(kPiece, a.n - t0);
     p.out = a.out + t0;
+    if (a.out2) p.out2 = a.out2 + t0;
     if (a.idx) p.idx = a.idx + t0;
     else p.g0 = (int32_t)(a.g0 + t0);
     p.ticket = qt ? tickets : ticket_slot(dev);
@@ -193,7 +194,7 @@ int run(bool aff, SwArgs a, cudaStream_t stream) {
     return status_of(cudaGetLastError());
   }
   if (!a.q) return SSEQS_ERR_ARG;
-  if (fast_domain(aff, a.p0, a.p1)) return launch_stream(a, aff, nullptr, stream);
+  if (fast_domain(aff, a.p0, a.p1)) return launch_stream(a, aff ? kAff : kLin, nullptr, stream);
   if (a.skip != 0) return SSEQS_ERR_UNSUPPORTED;
   const int grid = (int)std::min<int64_t>((a.n + 127) / 128, (int64_t)device_sm_count() * 4);
   { sw_generic_kernel<<<grid, 128, 0, stream>>>(a, aff ? 1 : 0); count_launches(1); }
@@ -298,6 +299,36 @@ extern "C" int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len
   return run(affine != 0, a, stream);
 }
 
+extern "C" int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len,
+                                  const int32_t* good_idx, int32_t g0, int64_t n_targets,
+                                  const uint8_t* ascii, const int32_t* delim, int affine_skip,
+                                  int32_t* out_linear, int32_t* out_affine, int gap,
+                                  int gap_open, int gap_extend, cudaStream_t stream) {
+  if (g0 < 0 || n_targets < 0 || (affine_skip != 0 && affine_skip != 1)) return SSEQS_ERR_ARG;
+  if (n_targets == 0) return SSEQS_OK;
+  if (!out_linear || !out_affine || !delim || !ascii || !query_idx) return SSEQS_ERR_ARG;
+  if (query_len < 1) return SSEQS_ERR_ARG;
+  if (query_len > kMaxQuery) return SSEQS_ERR_UNSUPPORTED;
+  if (!fast_domain(false, gap, 0) || !fast_domain(true, gap_open, gap_extend))
+    return SSEQS_ERR_UNSUPPORTED;
+  SwArgs a{query_idx, query_len, good_idx, g0, n_targets, ascii, delim, 0, out_linear, gap,
+           gap_open};
+  if ((query_len + 31) / 32 > kMaxFusedTpt) {   // no fused kernel: the two scans in turn
+    const int st = launch_stream(a, kLin, nullptr, stream);
+    if (st != SSEQS_OK) return st;
+    SwArgs b = a;
+    b.skip = affine_skip;
+    b.out = out_affine;
+    b.p0 = gap_open;
+    b.p1 = gap_extend;
+    return launch_stream(b, kAff, nullptr, stream);
+  }
+  a.p2 = gap_extend;
+  a.out2 = out_affine;
+  a.skip2 = affine_skip;
+  return launch_stream(a, kBoth, nullptr, stream);
+}
+
 extern "C" int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const uint8_t* queries,
                                      int64_t query_stride, const int32_t* query_lens,
                                      const int32_t* good_idx, int64_t idx_stride, int32_t g0,
@@ -325,7 +356,7 @@ extern "C" int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const u
     const int32_t* idx0 = good_idx ? good_idx + q0 * qt.idx_stride : nullptr;
     SwArgs a{queries + (size_t)q0 * query_stride, tpt * 32, idx0, g0, n_targets,
              ascii, delim, skip, out + q0 * out_stride, gap_a, gap_b, tickets + q0};
-    const int st = launch_stream(a, aff, &qt, stream);
+    const int st = launch_stream(a, aff ? kAff : kLin, &qt, stream);
     if (st != SSEQS_OK) return st;
   }
   return SSEQS_OK;
@@ -342,13 +373,14 @@ extern "C" int sseqs_int16x2_peak(uint32_t* sink, double* lane_ops_per_s, cudaSt
 }
 
 extern "C" int sseqs_sw_set_variant(int affine, int tpt, int wide) {
-  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1)) return SSEQS_ERR_ARG;
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine > 2)
+    return SSEQS_ERR_ARG;
   std::lock_guard<std::mutex> lk(cache().mu);
-  cache().variant[affine ? 1 : 0][tpt - 1] = wide;
+  cache().variant[affine][tpt - 1] = wide;
   return SSEQS_OK;
 }
 
 extern "C" int sseqs_sw_variant_words(int affine, int tpt, int wide) {
-  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1)) return -1;
-  return tables().k[wide][affine ? 1 : 0][tpt - 1].words;
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine > 2) return -1;
+  return tables().k[wide][affine][tpt - 1].words;
 }

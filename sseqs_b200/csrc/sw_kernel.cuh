@@ -56,9 +56,12 @@ constexpr int kMaxQuery = 2048;
 // (300k targets): affine 8 rows beat 4 by 10% at 27 words per lane, and 16
 // beat 8 by 2-3% at 16 words or fewer but lost 9% at 27 (larger code and
 // register footprint).  Linear 8 rows beat 4 by 3-7% where it fits, but
-// spills under the register caps of many widths, so linear keeps 4.
-template <bool AFF, int NWD>
-__host__ __device__ constexpr int rows_per_fetch() { return AFF ? (NWD <= 16 ? 16 : 8) : 4; }
+// spills under the register caps of many widths, so linear keeps 4, as
+// does the fused kernel (two states in registers).
+template <int MODE, int NWD>
+__host__ __device__ constexpr int rows_per_fetch() {
+  return MODE == 1 ? (NWD <= 16 ? 16 : 8) : 4;
+}
 
 struct SwArgs {
   const uint8_t* q;       // query residue classes
@@ -70,9 +73,13 @@ struct SwArgs {
   const int32_t* starts;  // window table (reference semantics)
   int skip;               // bytes not scored at the start of every window
   int32_t* out;
-  int p0, p1;             // linear: gap; affine: open, extend
+  int p0, p1;             // linear: gap; affine: open, extend; both: gap, open
   unsigned int* ticket;   // zeroed launch-wide target counter (fast kernel)
   int chunk;              // targets per counter grab (fast kernel, >= 1)
+  int p2;                 // both: extend
+  int32_t* out2;          // both: affine scores (out: linear)
+  int skip2;              // both: the affine windows start this many (0 or 1)
+                          // bytes after the linear ones
 };
 
 // Several queries of the same stripe width in one launch: blockIdx.y picks
@@ -147,64 +154,90 @@ struct Layout {
   static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
 };
 
+// Score variants of one instantiation: the linear kernel, the affine kernel,
+// or both in one pass over the targets (the exact search scores every
+// target with both; one pass shares the byte fetch, the per-row loads and
+// the bookkeeping, and lets the linear recurrence -- FMA-pipe heavy -- fill
+// the ALU pipe slack the affine one leaves, and vice versa).
+constexpr int kLin = 0, kAff = 1, kBoth = 2;
+
 // Block shape per instantiation.  The state of a lane is about NWD words
-// (linear: H; affine: D and Iy) plus its profile row, so registers grow
-// with NWD.  Up to ~128 registers a block has 8 warps that share one copy
-// of the query profile in shared memory, with the register cap set for 3
-// blocks (85 registers) or 2 (128) per SM; larger states use blocks of 4
-// warps, which pack the register file more finely.
-template <int TPT, int W, bool AFF>
+// (linear: H; affine: D and Iy; both: all three) plus its profile rows, so
+// registers grow with NWD.  Up to ~128 registers a block has 8 warps that
+// share one copy of the query profile in shared memory, with the register
+// cap set for 3 blocks (85 registers) or 2 (128) per SM; larger states use
+// blocks of 4 warps, which pack the register file more finely (the fused
+// kernel capped for 3 of them, 170 registers, when its estimate allows).
+template <int TPT, int W, int MODE>
 struct Shape {
   static constexpr int NWD = W * TPT;
-  static constexpr int est_regs = AFF ? 3 * NWD + 32 : 2 * NWD + 53;
+  static constexpr int est_regs = MODE == kAff ? 3 * NWD + 32
+                                : MODE == kLin ? 2 * NWD + 53 : 5 * NWD + 40;
   static constexpr int threads = est_regs <= 128 ? 256 : 128;
-  static constexpr int min_blocks = threads == 256 ? (est_regs <= 85 ? 3 : 2) : 1;
+  static constexpr int min_blocks =
+      threads == 256 ? (est_regs <= 85 ? 3 : 2)
+                     : (MODE == kBoth && est_regs <= 170 ? 3 : 1);
 };
 
-template <int TPT, int W, bool AFF>
-__global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF>::min_blocks)
+template <int TPT, int W, int MODE>
+__global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MODE>::min_blocks)
     sw_stream_kernel(SwArgs a, const QueryTable qt) {
   using L = Layout<TPT, W>;
+  constexpr bool DO_LIN = MODE != kAff, DO_AFF = MODE != kLin;
+  constexpr int NTAB = MODE == kBoth ? 2 : 1;
   if (qt.n > 0) {
     const int y = blockIdx.y;
     const int len = qt.lens[y];
     a.q += (size_t)y * qt.q_stride;
     a.out += (int64_t)y * qt.out_stride;
+    if constexpr (MODE == kBoth) a.out2 += (int64_t)y * qt.out_stride;
     if (a.idx) a.idx += (int64_t)y * qt.idx_stride;
     a.ticket += y;
     if (len < 1 || (len + 31) / 32 != TPT || len > qt.q_stride) {
       for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
-           i += (int64_t)gridDim.x * blockDim.x)
+           i += (int64_t)gridDim.x * blockDim.x) {
         a.out[i] = INT32_MIN;
+        if constexpr (MODE == kBoth) a.out2[i] = INT32_MIN;
+      }
       return;
     }
     a.Lq = len;
   }
   constexpr int G = L::G;
   extern __shared__ uint4 smem4[];
-  uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);
-  uint8_t* lut = reinterpret_cast<uint8_t*>(prof + kNumCls * L::CLS);
+  uint32_t* prof = reinterpret_cast<uint32_t*>(smem4);       // linear table first when both
+  uint8_t* lut = reinterpret_cast<uint8_t*>(prof + NTAB * kNumCls * L::CLS);
+
+  // Gap parameters: linear gap (p0); affine open and extend (p0, p1 in the
+  // affine kernel; p1, p2 in the fused one).
+  const int gap = a.p0;
+  const int open = MODE == kAff ? a.p0 : a.p1;
+  const int ext = MODE == kAff ? a.p1 : a.p2;
 
   // Profile words.  Affine: s (real columns), -32768 + open (padding), so
   // that M' - open never leaves int16.  Linear: s - gap (the state carries
   // H + gap), -16384 for padding.  Padding never raises a score.
-  const int pad = AFF ? kNeg + a.p0 : -16384;
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = ascii_class((uint8_t)i);
-  for (int i = threadIdx.x; i < kNumCls * L::CLS; i += blockDim.x) {
-    const int c = i / L::CLS, r = i - c * L::CLS;
+  for (int i = threadIdx.x; i < NTAB * kNumCls * L::CLS; i += blockDim.x) {
+    const int tb = i / (kNumCls * L::CLS), ii = i - tb * (kNumCls * L::CLS);
+    const bool aff_tab = MODE == kAff || tb == 1;
+    const int pad = aff_tab ? kNeg + open : -16384;
+    const int c = ii / L::CLS, r = ii - c * L::CLS;
     const int gl = r / L::LWP, v = r - gl * L::LWP;
     uint32_t word = pack2(pad, pad);
     if (v < L::NWD) {
       const int w = v / TPT, k = v - w * TPT;
       const int j = (gl * 2 * W + 2 * w) * TPT + k;
       int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + TPT);
-      s0 = (s0 == kNeg) ? pad : (AFF ? s0 : s0 - a.p0);
-      s1 = (s1 == kNeg) ? pad : (AFF ? s1 : s1 - a.p0);
+      s0 = (s0 == kNeg) ? pad : (aff_tab ? s0 : s0 - gap);
+      s1 = (s1 == kNeg) ? pad : (aff_tab ? s1 : s1 - gap);
       word = pack2(s0, s1);
     }
     prof[i] = word;
   }
   __syncthreads();
+  const uint32_t* profL = prof;
+  const uint32_t* profA = prof + (MODE == kBoth ? kNumCls * L::CLS : 0);
 
   const int lane = threadIdx.x & 31;
   const int grp = lane / G;
@@ -212,104 +245,126 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
   const int leader = grp * G;
 
-  const uint32_t gap2 = pack2(a.p0, a.p0);     // linear gap, -16384 <= gap <= 0
-  const uint32_t nopen2 = pack2(-a.p0, -a.p0); // affine -open, 0 <= open <= 16384
-  const uint32_t next2 = pack2(-a.p1, -a.p1);  // affine -extend, 0 <= extend <= 16384
+  const uint32_t gap2 = pack2(gap, gap);       // linear gap, -16384 <= gap <= 0
+  const uint32_t nopen2 = pack2(-open, -open); // affine -open, 0 <= open <= 16384
+  const uint32_t next2 = pack2(-ext, -ext);    // affine -extend, 0 <= extend <= 16384
   // state at row -1: H = 0 (linear state is H + gap), D = Iy = 0 (affine)
-  const uint32_t init = AFF ? 0u : gap2;
 
-  uint32_t S[W][TPT];                 // linear: H(i-1,.) + gap   affine: D(i-1,.)
-  uint32_t Y[AFF ? W : 1][TPT];       // affine: Iy(i,.) carried into row i
-  uint32_t best = 0;
+  constexpr int WL = DO_LIN ? W : 1, WA = DO_AFF ? W : 1;
+  uint32_t SL[WL][TPT];               // linear: H(i-1,.) + gap
+  uint32_t SA[WA][TPT];               // affine: D(i-1,.)
+  uint32_t Y[WA][TPT];                // affine: Iy(i,.) carried into row i
+  uint32_t bestL = 0, bestA = 0;
   auto reset = [&]() {
-    best = 0;
+    bestL = 0;
+    bestA = 0;
 #pragma unroll
     for (int w = 0; w < W; ++w)
 #pragma unroll
       for (int k = 0; k < TPT; ++k) {
-        S[w][k] = init;
-        if constexpr (AFF) Y[w][k] = 0;
+        if constexpr (DO_LIN) SL[w][k] = gap2;
+        if constexpr (DO_AFF) { SA[w][k] = 0; Y[w][k] = 0; }
       }
   };
   reset();
 
-  // one DP row for every group of the warp (warp-uniform)
-  auto row = [&](int cls) {
-    const uint4* pr = reinterpret_cast<const uint4*>(prof + cls * L::CLS + gl * L::LWP);
+  // one linear DP row for every group of the warp (warp-uniform)
+  auto row_lin = [&](int cls) {
+    const uint4* pr = reinterpret_cast<const uint4*>(profL + cls * L::CLS + gl * L::LWP);
     uint32_t s[L::NV * 4];
 #pragma unroll
     for (int v = 0; v < L::NV; ++v) {
       const uint4 x = pr[v];
       s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
-    uint32_t from_left = __shfl_up_sync(0xffffffffu, S[W - 1][TPT - 1], 1, G);
-    if (gl == 0) from_left = init;                  // column -1 of stripe 0
-    uint32_t din[W];
+    uint32_t from_left = __shfl_up_sync(0xffffffffu, SL[WL - 1][TPT - 1], 1, G);
+    if (gl == 0) from_left = gap2;                  // column -1 of stripe 0
+    uint32_t din[WL];                               // diagonals, from the previous row
 #pragma unroll
-    for (int w = 0; w < W; ++w)
-      din[w] = __byte_perm(w == 0 ? from_left : S[w - 1][TPT - 1], S[w][TPT - 1], 0x5432);
+    for (int w = 0; w < WL; ++w)
+      din[w] = __byte_perm(w == 0 ? from_left : SL[w - 1][TPT - 1], SL[w][TPT - 1], 0x5432);
     uint32_t pend = 0;
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-      uint32_t diag = din[w];
-      if constexpr (!AFF) {
-        // state Hg = H + gap:  H = max(Hg_diag + (s - gap), Hg_up, Hg_left, 0)
-        // (Hg_left = gap at the first column of a stripe).  The next
-        // column's diagonal sum is formed before S[k] is overwritten, so the
-        // new value can take the old one's register.
-        //
-        // The running maximum is taken over the diagonal sums u rather than
-        // over H: with gap <= 0 a cell whose H comes from Hg_up or Hg_left is
-        // never above the cell it came from, so following those moves back
-        // ends at a cell whose H is its u (or 0), and max H = max(0, max u).
-        // (Padding u lie 16384 below a real cell and never win.)  Taking
-        // the maximum over u keeps u a value of its own, so the compiler
-        // leaves its add on the FMA pipe instead of folding it into an
-        // add-max on the ALU pipe, which is the busier one.
-        uint32_t hg_left = 0;
-        uint32_t u = __vadd2(diag, s[w * TPT]);                             // FMA pipe
+    for (int w = 0; w < WL; ++w) {
+      const uint32_t diag = din[w];
+      // state Hg = H + gap:  H = max(Hg_diag + (s - gap), Hg_up, Hg_left, 0)
+      // (Hg_left = gap at the first column of a stripe).  The next column's
+      // diagonal sum is formed before S[k] is overwritten, so the new value
+      // can take the old one's register.
+      //
+      // The running maximum is taken over the diagonal sums u rather than
+      // over H: with gap <= 0 a cell whose H comes from Hg_up or Hg_left is
+      // never above the cell it came from, so following those moves back
+      // ends at a cell whose H is its u (or 0), and max H = max(0, max u).
+      // (Padding u lie 16384 below a real cell and never win.)  Taking the
+      // maximum over u keeps u a value of its own, so the compiler leaves
+      // its add on the FMA pipe instead of folding it into an add-max on the
+      // ALU pipe, which is the busier one.
+      uint32_t hg_left = 0;
+      uint32_t u = __vadd2(diag, s[w * TPT]);                               // FMA pipe
 #pragma unroll
-        for (int k = 0; k < TPT; ++k) {
-          const uint32_t up = S[w][k];
-          const uint32_t u_next = (k + 1 < TPT) ? __vadd2(up, s[w * TPT + k + 1]) : 0u;
-          const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
-                                      : __vimax3_s16x2_relu(u, up, hg_left); // ALU pipe
-          hg_left = __vadd2(h, gap2);                                       // FMA pipe
-          S[w][k] = hg_left;
-          if (((w * TPT + k) & 1) == 0) pend = u;
-          else best = __vimax3_s16x2(best, pend, u);
-          u = u_next;
-        }
-      } else {
-        // M' = D_diag + s (unclamped), Mo = M' - open          FMA pipe
-        // Ix = max(Ix_left - ext, Mo_left, 0)   (0 at k = 0)  ALU
-        // D  = max(M', Ix, Iy, 0)                             ALU
-        // Iy(next row) = max(Iy - ext, Mo, 0)                 ALU
-        uint32_t X = 0, mo_left = 0;
-        uint32_t mp = __vadd2(diag, s[w * TPT]);
-#pragma unroll
-        for (int k = 0; k < TPT; ++k) {
-          const uint32_t mo = __vadd2(mp, nopen2);
-          const uint32_t mp_next = (k + 1 < TPT) ? __vadd2(S[w][k], s[w * TPT + k + 1]) : 0u;
-          if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
-          const uint32_t y = Y[w][k];
-          const uint32_t D = (k > 0) ? __vimax3_s16x2_relu(mp, X, y) : __vimax_s16x2_relu(mp, y);
-          Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
-          S[w][k] = D;
-          mo_left = mo;
-          mp = mp_next;
-          if (((w * TPT + k) & 1) == 0) pend = D;
-          else best = __vimax3_s16x2(best, pend, D);
-        }
+      for (int k = 0; k < TPT; ++k) {
+        const uint32_t up = SL[w][k];
+        const uint32_t u_next = (k + 1 < TPT) ? __vadd2(up, s[w * TPT + k + 1]) : 0u;
+        const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
+                                    : __vimax3_s16x2_relu(u, up, hg_left);   // ALU pipe
+        hg_left = __vadd2(h, gap2);                                         // FMA pipe
+        SL[w][k] = hg_left;
+        if (((w * TPT + k) & 1) == 0) pend = u;
+        else bestL = __vimax3_s16x2(bestL, pend, u);
+        u = u_next;
       }
     }
-    if ((L::NWD & 1) != 0) best = __vimax_s16x2_relu(best, pend);
+    if ((L::NWD & 1) != 0) bestL = __vimax_s16x2_relu(bestL, pend);
+  };
+
+  // one affine DP row for every group of the warp (warp-uniform)
+  auto row_aff = [&](int cls) {
+    const uint4* pr = reinterpret_cast<const uint4*>(profA + cls * L::CLS + gl * L::LWP);
+    uint32_t s[L::NV * 4];
+#pragma unroll
+    for (int v = 0; v < L::NV; ++v) {
+      const uint4 x = pr[v];
+      s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
+    }
+    uint32_t from_left = __shfl_up_sync(0xffffffffu, SA[WA - 1][TPT - 1], 1, G);
+    if (gl == 0) from_left = 0u;                    // column -1 of stripe 0
+    uint32_t din[WA];                               // diagonals, from the previous row
+#pragma unroll
+    for (int w = 0; w < WA; ++w)
+      din[w] = __byte_perm(w == 0 ? from_left : SA[w - 1][TPT - 1], SA[w][TPT - 1], 0x5432);
+    uint32_t pend = 0;
+#pragma unroll
+    for (int w = 0; w < WA; ++w) {
+      const uint32_t diag = din[w];
+      // M' = D_diag + s (unclamped), Mo = M' - open          FMA pipe
+      // Ix = max(Ix_left - ext, Mo_left, 0)   (0 at k = 0)  ALU
+      // D  = max(M', Ix, Iy, 0)                             ALU
+      // Iy(next row) = max(Iy - ext, Mo, 0)                 ALU
+      uint32_t X = 0, mo_left = 0;
+      uint32_t mp = __vadd2(diag, s[w * TPT]);
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) {
+        const uint32_t mo = __vadd2(mp, nopen2);
+        const uint32_t mp_next = (k + 1 < TPT) ? __vadd2(SA[w][k], s[w * TPT + k + 1]) : 0u;
+        if (k > 0) X = __viaddmax_s16x2_relu(X, next2, mo_left);
+        const uint32_t y = Y[w][k];
+        const uint32_t D = (k > 0) ? __vimax3_s16x2_relu(mp, X, y) : __vimax_s16x2_relu(mp, y);
+        Y[w][k] = __viaddmax_s16x2_relu(y, next2, mo);
+        SA[w][k] = D;
+        mo_left = mo;
+        mp = mp_next;
+        if (((w * TPT + k) & 1) == 0) pend = D;
+        else bestA = __vimax3_s16x2(bestA, pend, D);
+      }
+    }
+    if ((L::NWD & 1) != 0) bestA = __vimax_s16x2_relu(bestA, pend);
   };
 
   // ---- target bytes: R rows at a time from R/4 + 1 aligned 32-bit words.
   // A word is loaded only when it holds a byte of the window being read, so
   // no load leaves the windows' own 4-byte words.
-  constexpr int R = rows_per_fetch<AFF, L::NWD>();
+  constexpr int R = rows_per_fetch<MODE, L::NWD>();
   constexpr int NWORDS = R / 4 + 1;
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
@@ -324,12 +379,18 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
       q.w[k] = ((wi + k) << 2) < e + aoff ? __ldg(abase + wi + k) : 0u;
     return q;
   };
-  // residue classes of the next R rows, four 8-bit classes per word
+  // residue classes of the next R rows, four 8-bit classes per word; in the
+  // fused kernel the affine rows may differ from the linear ones in the
+  // first row of a target, which is a padding row when the affine windows
+  // start one byte later (a padding row from the initial state leaves the
+  // state at 0, so this is exactly the later start)
   constexpr uint32_t kPadWord = kClsPad * 0x01010101u;
+  const bool aff_skip_row = MODE == kBoth && a.skip2 == 1;
   uint32_t cw[R / 4];
+  uint32_t cwa0 = kPadWord;           // fused kernel: affine classes of rows 0-3
 #pragma unroll
   for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
-  auto classes = [&](const Bytes& q, uint32_t p, uint32_t e) {
+  auto classes = [&](const Bytes& q, uint32_t p, uint32_t e, bool first) {
     const uint32_t sh = ((p + aoff) & 3u) * 8u;
 #pragma unroll
     for (int h = 0; h < R / 4; ++h) {
@@ -342,6 +403,8 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
       }
       cw[h] = word;
     }
+    if constexpr (MODE == kBoth)
+      cwa0 = (first && aff_skip_row) ? ((cw[0] & 0xffffff00u) | kClsPad) : cw[0];
   };
 
   // ---- target order (group-uniform).  The group leader takes CH targets
@@ -376,7 +439,10 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
     while (t < n) {
       cur = window_of(a, t);
       if (cur.rows) break;
-      if (gl == 0) a.out[t] = cur.res;
+      if (gl == 0) {
+        a.out[t] = cur.res;
+        if constexpr (MODE == kBoth) a.out2[t] = cur.res;
+      }
       t = successor(t);
     }
     active = t < n;
@@ -386,9 +452,15 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
       if (tn < n) { nxt = window_of(a, tn); nxt_ok = true; }
     }
   };
+  auto finish = [&](uint32_t best) -> int {   // group maximum of a running max
+    int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
+    return v;
+  };
   issue_grab();
   start_at(take_chunk());
-  if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
+  if (active) classes(fetch(cur.pos, cur.end), cur.pos, cur.end, true);
 
   while (__any_sync(0xffffffffu, active)) {
     // prefetch the bytes of the next R rows of this group
@@ -399,15 +471,23 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
       else if (nxt_ok && nxt.rows) { pf = fetch(nxt.pos, nxt.end); pf_nxt = true; }
     }
 #pragma unroll
-    for (int r = 0; r < R; ++r) row((int)((cw[r / 4] >> (8 * (r % 4))) & 0xffu));
+    for (int r = 0; r < R; ++r) {
+      const int cl = (int)((cw[r / 4] >> (8 * (r % 4))) & 0xffu);
+      if constexpr (DO_LIN) row_lin(cl);
+      if constexpr (MODE == kAff) row_aff(cl);
+      if constexpr (MODE == kBoth) row_aff(r < 4 ? (int)((cwa0 >> (8 * r)) & 0xffu) : cl);
+    }
     if (active) {
       cur.pos += R;
       if (cur.pos >= cur.end) {
         // target finished (rows past its end were padding rows)
-        int v = max((int)(int16_t)(best & 0xffffu), (int)(int16_t)(best >> 16));
-#pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
-        if (gl == 0) a.out[t] = v;
+        const int vl = DO_LIN ? finish(bestL) : 0;
+        const int va = DO_AFF ? finish(bestA) : 0;
+        if (gl == 0) {
+          if constexpr (MODE == kLin) a.out[t] = vl;
+          if constexpr (MODE == kAff) a.out[t] = va;
+          if constexpr (MODE == kBoth) { a.out[t] = vl; a.out2[t] = va; }
+        }
         reset();
         if (pf_nxt) {
           t = tn;
@@ -415,18 +495,19 @@ __global__ void __launch_bounds__(Shape<TPT, W, AFF>::threads, Shape<TPT, W, AFF
           tn = successor(t);
           nxt_ok = tn < n;
           if (nxt_ok) nxt = window_of(a, tn);
-          classes(pf, cur.pos, cur.end);
+          classes(pf, cur.pos, cur.end, true);
         } else {
           start_at(tn);
           if (active) {
-            classes(fetch(cur.pos, cur.end), cur.pos, cur.end);
+            classes(fetch(cur.pos, cur.end), cur.pos, cur.end, true);
           } else {
 #pragma unroll
             for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
+            cwa0 = kPadWord;
           }
         }
       } else {
-        classes(pf, cur.pos, cur.end);
+        classes(pf, cur.pos, cur.end, false);
       }
     }
   }
@@ -443,27 +524,40 @@ struct KernelInfo {
   int words = 0;
 };
 
-template <int TPT, bool AFF, bool WIDE>
+template <int TPT, int MODE, bool WIDE>
 KernelInfo make_info() {
   constexpr int W = words_for<TPT, WIDE>();
   KernelInfo k;
-  k.fn = sw_stream_kernel<TPT, W, AFF>;
-  k.smem = Layout<TPT, W>::smem;
-  k.threads = Shape<TPT, W, AFF>::threads;
+  k.fn = sw_stream_kernel<TPT, W, MODE>;
+  k.smem = Layout<TPT, W>::smem + (MODE == kBoth ? Layout<TPT, W>::smem - 256 : 0);
+  k.threads = Shape<TPT, W, MODE>::threads;
   k.groups_per_block = (k.threads / 32) * Layout<TPT, W>::GPW;
   k.words = W;
   return k;
 }
 
-// tables[variant][affine][TPT - 1], variant 0 = narrow, 1 = wide
+// tables[variant][mode][TPT - 1], variant 0 = narrow, 1 = wide;
+// mode kLin, kAff or kBoth.  The fused kernel exists up to kMaxFusedTpt;
+// wider queries run the two kernels one after the other (fn == nullptr
+// here).  Measured on B200 over 1M segments, the fused pass beat the two
+// kernels by 4-17% up to 16 words per lane but lost 4% at 22-27 and 13% at
+// 41-48: its three states need ~200-255 registers there, which leaves 8
+// warps per SM instead of 16.
+constexpr int kMaxFusedTpt = 16;
 struct Tables {
-  KernelInfo k[2][2][64];
+  KernelInfo k[2][3][64];
 };
+
+template <int T, bool WIDE>
+void fill_one(Tables& t) {
+  t.k[WIDE][kLin][T - 1] = make_info<T, kLin, WIDE>();
+  t.k[WIDE][kAff][T - 1] = make_info<T, kAff, WIDE>();
+  if constexpr (T <= kMaxFusedTpt) t.k[WIDE][kBoth][T - 1] = make_info<T, kBoth, WIDE>();
+}
 
 template <int LO, bool WIDE, int... I>
 void fill_range(Tables& t, std::integer_sequence<int, I...>) {
-  ((t.k[WIDE][0][LO + I - 1] = make_info<LO + I, false, WIDE>()), ...);
-  ((t.k[WIDE][1][LO + I - 1] = make_info<LO + I, true, WIDE>()), ...);
+  (fill_one<LO + I, WIDE>(t), ...);
 }
 
 // Defined in the instantiation units sw_inst_*.cu.

@@ -30,7 +30,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import select
+from . import select, tune
 from ._lib import check, lib, ptr, stream_ptr, to_host
 from .database import Database, default_database
 from .to_a3m import to_a3m
@@ -88,30 +88,42 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
         scores = conv.prefilter_batch(query, batch, luts, fft_rank)
         cand = select.topk_indices(scores, k1)[1:-1]
     Lq = q_enc.numel()
-    if cand is None:
-        lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, g0=1, n_targets=n_c,
-                          skip=0, gap_a=-1)
-    else:
-        lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, good_idx=cand,
-                          skip=0, gap_a=-1)
     k2 = n_c // top_sw
-    if k2 <= 0:
-        return None
-    if top_sw == 1:
+    if top_sw == 1 and tune.fused(Lq):
+        # every candidate gets both scores: one fused pass (same scores as
+        # the two calls below)
+        if timer is not None:
+            timer("both", True)
+        tgt = dict(g0=1, n_targets=n_c) if cand is None else dict(good_idx=cand)
+        lin, aff = _sw.sw_scan_both(q_enc, batch.ascii, batch.delim, affine_skip=1, gap=-1,
+                                    gap_open=11, gap_extend=1, **tgt)
+        if timer is not None:
+            timer("both", False)
         p2, cand2 = None, cand
     else:
-        p2 = select.topk_indices(lin, k2)
-        cand2 = (p2 + 1) if cand is None else cand[p2.long()]
-    if timer is not None:
-        timer("affine", True)
-    if cand2 is None:
-        aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, g0=1, n_targets=k2,
-                          skip=1, gap_a=11, gap_b=1)
-    else:
-        aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, good_idx=cand2,
-                          skip=1, gap_a=11, gap_b=1)
-    if timer is not None:
-        timer("affine", False)
+        if cand is None:
+            lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, g0=1,
+                              n_targets=n_c, skip=0, gap_a=-1)
+        else:
+            lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, good_idx=cand,
+                              skip=0, gap_a=-1)
+        if k2 <= 0:
+            return None
+        if top_sw == 1:
+            p2, cand2 = None, cand
+        else:
+            p2 = select.topk_indices(lin, k2)
+            cand2 = (p2 + 1) if cand is None else cand[p2.long()]
+        if timer is not None:
+            timer("affine", True)
+        if cand2 is None:
+            aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, g0=1, n_targets=k2,
+                              skip=1, gap_a=11, gap_b=1)
+        else:
+            aff = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=True, good_idx=cand2,
+                              skip=1, gap_a=11, gap_b=1)
+        if timer is not None:
+            timer("affine", False)
     # torch.topk raises when top_sw_affine exceeds the list (msa.py:335);
     # here the list is kept whole instead.
     k3 = min(top_sw_affine, k2)

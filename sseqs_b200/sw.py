@@ -88,6 +88,27 @@ def sw_scan(query_idx: torch.Tensor, ascii: torch.Tensor, delim: torch.Tensor, *
     return out
 
 
+def sw_scan_both(query_idx: torch.Tensor, ascii: torch.Tensor, delim: torch.Tensor, *,
+                 good_idx: torch.Tensor | None = None, g0: int = 0,
+                 n_targets: int | None = None, affine_skip: int = 1, gap: int = -1,
+                 gap_open: int = 11, gap_extend: int = 1):
+    """Linear (windows of ``sw_scan`` with skip 0) and affine (windows
+    ``affine_skip`` bytes later) scores of the same targets in one pass:
+    returns ``(linear, affine)``, each equal to its own ``sw_scan`` call."""
+    if good_idx is not None:
+        good_idx = _i32(good_idx)
+        n = good_idx.numel()
+    else:
+        n = int(n_targets)
+    lin = torch.empty(n, dtype=torch.int32, device=ascii.device)
+    aff = torch.empty(n, dtype=torch.int32, device=ascii.device)
+    check(lib().sseqs_sw_scan_both(ptr(query_idx), query_idx.numel(), ptr(good_idx), int(g0), n,
+                                   ptr(ascii), ptr(delim), int(affine_skip), ptr(lin), ptr(aff),
+                                   int(gap), int(gap_open), int(gap_extend), stream_ptr()),
+          "sw_scan_both")
+    return lin, aff
+
+
 def encode_query(query: str, device="cuda") -> torch.Tensor:
     """Class indices of the standard residues of ``query`` (sseqs/sw.py:11)."""
     return to_device(torch.tensor([AA_MAP[c] for c in query if c in AA_MAP], dtype=torch.uint8),

@@ -161,3 +161,73 @@ def test_wide_layout_matches_oracle(Lq):
     finally:
         tune.set_variant(False, tpt, 0)
         tune.set_variant(True, tpt, 0)
+
+
+
+def _set_variant(mode, tpt, wide):
+    from sseqs_b200 import _lib
+    _lib.check(_lib.lib().sseqs_sw_set_variant(mode, tpt, wide), "set_variant")
+
+
+@pytest.mark.parametrize("Lq", [1, 20, 33, 64, 100, 200, 287, 500, 545, 858, 1000, 1300, 1536,
+                                1537, 2048])
+@pytest.mark.parametrize("wide", [0, 1])
+def test_scan_both_equals_two_scans(Lq, wide):
+    """The fused pass gives exactly the linear (skip 0) and affine (skip 1 or
+    0) scores of the two separate scans and of the oracle; widths above 48
+    words run the two kernels in turn."""
+    S = importlib.import_module("sseqs_b200.sw")
+    tpt = (Lq + 31) // 32
+    if wide and tpt > 16:
+        pytest.skip("the wide layout exists for widths up to 16")
+    n = 500 if Lq <= 300 else 160
+    query, q, ascii, starts = _case(Lq + 3, Lq, n, extra="XBZU*")
+    ascii = np.concatenate([ascii, np.full(40, 64, np.uint8)])
+    delim = np.flatnonzero(ascii == 64).astype(np.int32)
+    nseg = len(delim)
+    qd, ad, dd = _dev(q), _dev(ascii), _dev(delim)
+    for mode in (0, 1, 2):
+        _set_variant(mode, tpt, wide)
+    try:
+        lin, aff = S.sw_scan_both(qd, ad, dd, g0=1, n_targets=nseg - 1, affine_skip=1)
+        exp_l = S.sw_scan(qd, ad, dd, affine=False, g0=1, n_targets=nseg - 1, skip=0, gap_a=-1)
+        exp_a = S.sw_scan(qd, ad, dd, affine=True, g0=1, n_targets=nseg - 1, skip=1, gap_a=11,
+                          gap_b=1)
+        torch.testing.assert_close(lin, exp_l, rtol=0, atol=0)
+        torch.testing.assert_close(aff, exp_a, rtol=0, atol=0)
+        good = np.arange(1, nseg, dtype=np.int32)
+        np.testing.assert_array_equal(lin.cpu().numpy(),
+                                      O.sw_linear(q, good, ascii, delim, -1, NT))
+        np.testing.assert_array_equal(aff.cpu().numpy(),
+                                      O.sw_affine(q, good, ascii, delim + 1, 11, 1, NT))
+        # explicit order with repeats, other gaps, affine windows not shifted
+        rng = np.random.default_rng(Lq)
+        idx = rng.integers(1, nseg, 300).astype(np.int32)
+        gd = _dev(idx)
+        lin2, aff2 = S.sw_scan_both(qd, ad, dd, good_idx=gd, affine_skip=0, gap=-2, gap_open=7,
+                                    gap_extend=2)
+        torch.testing.assert_close(lin2, S.sw_scan(qd, ad, dd, affine=False, good_idx=gd, skip=0,
+                                                   gap_a=-2), rtol=0, atol=0)
+        torch.testing.assert_close(aff2, S.sw_scan(qd, ad, dd, affine=True, good_idx=gd, skip=0,
+                                                   gap_a=7, gap_b=2), rtol=0, atol=0)
+    finally:
+        for mode in (0, 1, 2):
+            _set_variant(mode, tpt, 0)
+
+
+def test_scan_both_degenerate_windows():
+    """Empty, one-residue and inverted windows (decreasing delimiters), and
+    g = 0, in the fused pass."""
+    S = importlib.import_module("sseqs_b200.sw")
+    qs = "MKTAYIAKQRQISFVKSHFSRQ"
+    q = _dev(O.encode_query(qs))
+    ascii = np.frombuffer(b"MKTAYIAK@@QRQ@W@AKQRQISF@", np.uint8).copy()
+    delim = np.array([8, 9, 13, 15, 15, 3, 24, 24, 0, 20], np.int32)
+    ad, dd = _dev(ascii), _dev(delim)
+    idx = _dev(np.arange(len(delim), dtype=np.int32))
+    for skip in (0, 1):
+        lin, aff = S.sw_scan_both(q, ad, dd, good_idx=idx, affine_skip=skip)
+        torch.testing.assert_close(lin, S.sw_scan(q, ad, dd, affine=False, good_idx=idx, skip=0,
+                                                  gap_a=-1), rtol=0, atol=0)
+        torch.testing.assert_close(aff, S.sw_scan(q, ad, dd, affine=True, good_idx=idx,
+                                                  skip=skip, gap_a=11, gap_b=1), rtol=0, atol=0)
