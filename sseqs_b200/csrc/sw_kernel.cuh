@@ -58,9 +58,9 @@ constexpr int kMaxQuery = 2048;
 // register footprint).  Linear 8 rows beat 4 by 3-7% where it fits, but
 // spills under the register caps of many widths, so linear keeps 4, as
 // does the fused kernel (two states in registers).
-template <int MODE, int NWD>
+template <int MODE, int TPT, int W>
 __host__ __device__ constexpr int rows_per_fetch() {
-  return MODE == 1 ? (NWD <= 16 ? 16 : 8) : 4;
+  return MODE == 1 ? (W * TPT <= 16 ? 16 : 8) : 4;
 }
 
 struct SwArgs {
@@ -136,9 +136,15 @@ __device__ __forceinline__ int score_of(const uint8_t* q, int Lq, int cls, int j
 // Words per lane for a stripe width: the narrow variant keeps a target on
 // 16 lanes down to TPT 9 and widens below; the wide variant gives each lane
 // twice the columns (fewer lanes per target, more targets per warp) for
-// TPT <= 16.  The choice per width is made by the autotuner at run time.
-template <int TPT, bool WIDE>
+// TPT <= 16, and for the linear kernel up to TPT 29 (two independent
+// recurrence chains per lane; measured on B200 it beat the narrow layout by
+// 7-11% at widths 20-27, where the linear kernel waits on the latency of
+// its one chain; the affine kernel, bound by its ALU pipe, lost 1-20%).
+// Wide equals narrow where no wide layout exists.  The choice per width is
+// made by the autotuner at run time.
+template <int TPT, bool WIDE, int MODE>
 constexpr int words_for() {
+  if (WIDE && MODE == 0 && TPT > 16 && TPT <= 29) return 2;
   if (WIDE) return TPT == 1 ? 16 : TPT == 2 ? 16 : TPT <= 4 ? 8 : TPT <= 8 ? 4 : TPT <= 16 ? 2 : 1;
   return TPT == 1 ? 16 : TPT == 2 ? 8 : TPT <= 4 ? 4 : TPT <= 8 ? 2 : 1;
 }
@@ -176,7 +182,8 @@ struct Shape {
   static constexpr int threads = est_regs <= 128 ? 256 : 128;
   static constexpr int min_blocks =
       threads == 256 ? (est_regs <= 85 ? 3 : 2)
-                     : (MODE == kBoth && est_regs <= 170 ? 3 : 1);
+                     : ((MODE == kBoth || (MODE == kLin && TPT > 16 && W == 2)) &&
+                        est_regs <= 170 ? 3 : 1);
 };
 
 template <int TPT, int W, int MODE>
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   // ---- target bytes: R rows at a time from R/4 + 1 aligned 32-bit words.
   // A word is loaded only when it holds a byte of the window being read, so
   // no load leaves the windows' own 4-byte words.
-  constexpr int R = rows_per_fetch<MODE, L::NWD>();
+  constexpr int R = rows_per_fetch<MODE, TPT, W>();
   constexpr int NWORDS = R / 4 + 1;
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
@@ -526,7 +533,7 @@ struct KernelInfo {
 
 template <int TPT, int MODE, bool WIDE>
 KernelInfo make_info() {
-  constexpr int W = words_for<TPT, WIDE>();
+  constexpr int W = words_for<TPT, WIDE, MODE>();
   KernelInfo k;
   k.fn = sw_stream_kernel<TPT, W, MODE>;
   k.smem = Layout<TPT, W>::smem + (MODE == kBoth ? Layout<TPT, W>::smem - 256 : 0);

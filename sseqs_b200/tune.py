@@ -1,8 +1,9 @@
 """Autotuner of the score kernel's lane layout.
 
-For every stripe width tpt = ceil(query_len/32) <= 16 the score kernel exists
-in two layouts (see ``sseqs_sw_set_variant``): fewer, longer rows per lane
-group, or more targets per warp with twice the columns per lane.  Both give
+For every stripe width tpt = ceil(query_len/32) <= 16 (linear kernel: <= 29)
+the score kernel exists in two layouts (see ``sseqs_sw_set_variant``): fewer,
+longer rows per lane group, or more targets per warp with twice the columns
+per lane.  Both give
 identical scores; which is faster depends on the width and on register
 pressure, so it is measured: each candidate scores a sample of database
 segments, timed with CUDA events on the current stream, and the faster one is
@@ -31,6 +32,12 @@ MAX_FUSED_TPT = 16      # widths scored by the fused pass (wider: the two kernel
 def set_variant(affine, tpt: int, wide: int) -> None:
     """``affine``: False/0 linear, True/1 affine, 2 the fused pass."""
     check(lib().sseqs_sw_set_variant(int(affine), int(tpt), int(wide)), "set_variant")
+
+
+def has_wide(mode: int, tpt: int) -> bool:
+    """Whether the kernel of ``mode`` has a wide layout of its own at ``tpt``."""
+    words = [lib().sseqs_sw_variant_words(int(mode), int(tpt), w) for w in (0, 1)]
+    return words[0] > 0 and words[1] != words[0]
 
 
 def fused(query_len: int) -> bool:
@@ -74,12 +81,14 @@ def autotune(query_lengths, batch, max_segments: int = 200_000, reps: int = 2) -
     gen = torch.Generator(device="cpu")
     gen.manual_seed(1)
     for tpt in sorted({tpt_of(L) for L in query_lengths if 0 < L}):
-        if tpt > 16:
-            continue
-        q = torch.randint(0, 20, (tpt * 32,), generator=gen, dtype=torch.uint8).cuda()
+        q = None
         for mode, name in enumerate(MODES):
             if (name, tpt) in _chosen or (mode == 2 and tpt > MAX_FUSED_TPT):
                 continue
+            if not has_wide(mode, tpt):
+                continue
+            if q is None:
+                q = torch.randint(0, 20, (tpt * 32,), generator=gen, dtype=torch.uint8).cuda()
             t = []
             for wide in (0, 1):
                 set_variant(mode, tpt, wide)

@@ -139,7 +139,7 @@ def test_sw_api_matches_oracle():
     np.testing.assert_array_equal(got, exp)
 
 
-@pytest.mark.parametrize("Lq", [17, 40, 100, 200, 300, 500])
+@pytest.mark.parametrize("Lq", [17, 40, 100, 200, 300, 500, 513, 600, 700, 858, 928, 929])
 def test_wide_layout_matches_oracle(Lq):
     """Both lane layouts of a stripe width give the oracle's scores."""
     S = importlib.import_module("sseqs_b200.sw")
