@@ -37,8 +37,9 @@
 // counter (a few at a time, the next grab issued one chunk ahead so its
 // latency is hidden), which keeps every group busy until the last targets
 // whatever their lengths.  A target is read R rows at a time (4, 8 or 16,
-// see rows_per_fetch), the R bytes of the next step prefetched with R/4 + 1 aligned
-// 32-bit loads; when a target ends (rows past its end are padding rows) the
+// see rows_per_fetch), the R bytes of the next step prefetched (one byte per
+// lane, or R/4 + 1 aligned words per lane in groups of fewer than R lanes);
+// when a target ends (rows past its end are padding rows) the
 // group writes its score, resets its state and moves on while the other
 // groups of the warp keep going.
 #pragma once
@@ -372,46 +373,67 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   // A word is loaded only when it holds a byte of the window being read, so
   // no load leaves the windows' own 4-byte words.
   constexpr int R = rows_per_fetch<MODE, TPT, W>();
-  constexpr int NWORDS = R / 4 + 1;
+  // ---- target bytes and residue classes of the next R rows.  Only bytes
+  // inside the window are read; rows past its end are padding rows (class
+  // kClsPad).  Where a group has at least R lanes (SPREAD), the lanes share
+  // the work: lane gl reads the byte of row gl and turns it into a class,
+  // and each row's class is broadcast from its lane with one shuffle (LSU
+  // pipe), which keeps the per-byte work off the busy ALU pipe.  Narrower
+  // groups read R/4 + 1 aligned 32-bit words per lane, a word only when it
+  // holds a byte of the window, and pack four classes per register.
+  constexpr bool SPREAD = G >= R;
+  constexpr int NB = SPREAD ? 1 : R / 4 + 1;   // bytes (SPREAD) or words per lane
+  constexpr uint32_t kNoByte = 0x100u;         // SPREAD: the row is past the end
+  constexpr uint32_t kPadWord = kClsPad * 0x01010101u;
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
   const uint32_t aoff = (uint32_t)(au & 3);
-  struct Bytes { uint32_t w[NWORDS]; };
+  struct Bytes { uint32_t w[NB]; };
   auto fetch = [&](uint32_t p, uint32_t e) -> Bytes {   // needs p < e
-    const uint32_t wi = (p + aoff) >> 2;
     Bytes q;
-    q.w[0] = __ldg(abase + wi);
+    if constexpr (SPREAD) {
+      q.w[0] = (gl < R && p + (uint32_t)gl < e) ? (uint32_t)__ldg(a.ascii + p + gl) : kNoByte;
+    } else {
+      const uint32_t wi = (p + aoff) >> 2;
+      q.w[0] = __ldg(abase + wi);
 #pragma unroll
-    for (int k = 1; k < NWORDS; ++k)
-      q.w[k] = ((wi + k) << 2) < e + aoff ? __ldg(abase + wi + k) : 0u;
+      for (int k = 1; k < NB; ++k)
+        q.w[k] = ((wi + k) << 2) < e + aoff ? __ldg(abase + wi + k) : 0u;
+    }
     return q;
   };
-  // residue classes of the next R rows, four 8-bit classes per word; in the
-  // fused kernel the affine rows may differ from the linear ones in the
-  // first row of a target, which is a padding row when the affine windows
-  // start one byte later (a padding row from the initial state leaves the
-  // state at 0, so this is exactly the later start)
-  constexpr uint32_t kPadWord = kClsPad * 0x01010101u;
+  // In the fused kernel the affine rows may differ from the linear ones in
+  // the first row of a target, which is a padding row when the affine
+  // windows start one byte later (a padding row from the initial state
+  // leaves the state at 0, so this is exactly the later start).
   const bool aff_skip_row = MODE == kBoth && a.skip2 == 1;
-  uint32_t cw[R / 4];
-  uint32_t cwa0 = kPadWord;           // fused kernel: affine classes of rows 0-3
+  constexpr int NC = SPREAD ? 1 : R / 4;
+  uint32_t cw[NC];                    // SPREAD: class of row gl; else 4 per word
+  bool pad0 = false;                  // fused kernel: affine row 0 is padding
 #pragma unroll
-  for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
+  for (int h = 0; h < NC; ++h) cw[h] = SPREAD ? (uint32_t)kClsPad : kPadWord;
   auto classes = [&](const Bytes& q, uint32_t p, uint32_t e, bool first) {
-    const uint32_t sh = ((p + aoff) & 3u) * 8u;
+    if constexpr (SPREAD) {
+      cw[0] = q.w[0] < 256u ? (uint32_t)lut[q.w[0]] : (uint32_t)kClsPad;
+    } else {
+      const uint32_t sh = ((p + aoff) & 3u) * 8u;
 #pragma unroll
-    for (int h = 0; h < R / 4; ++h) {
-      const uint32_t raw = __funnelshift_r(q.w[h], q.w[h + 1], sh);
-      uint32_t word = 0;
+      for (int h = 0; h < NC; ++h) {
+        const uint32_t raw = __funnelshift_r(q.w[h], q.w[h + 1], sh);
+        uint32_t word = 0;
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const uint32_t cl = p + (4 * h + b) < e ? lut[(raw >> (8 * b)) & 0xffu] : kClsPad;
-        word |= cl << (8 * b);
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t cl = p + (4 * h + b) < e ? lut[(raw >> (8 * b)) & 0xffu] : kClsPad;
+          word |= cl << (8 * b);
+        }
+        cw[h] = word;
       }
-      cw[h] = word;
     }
-    if constexpr (MODE == kBoth)
-      cwa0 = (first && aff_skip_row) ? ((cw[0] & 0xffffff00u) | kClsPad) : cw[0];
+    if constexpr (MODE == kBoth) pad0 = first && aff_skip_row;
+  };
+  auto class_of_row = [&](int r) -> int {
+    if constexpr (SPREAD) return __shfl_sync(0xffffffffu, (int)cw[0], leader + r);
+    else return (int)((cw[r / 4] >> (8 * (r % 4))) & 0xffu);
   };
 
   // ---- target order (group-uniform).  The group leader takes CH targets
@@ -471,7 +493,9 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
 
   while (__any_sync(0xffffffffu, active)) {
     // prefetch the bytes of the next R rows of this group
-    Bytes pf{};
+    Bytes pf;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) pf.w[k] = SPREAD ? kNoByte : 0u;
     bool pf_nxt = false;
     if (active) {
       if (cur.pos + R < cur.end) pf = fetch(cur.pos + R, cur.end);
@@ -479,10 +503,10 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int cl = (int)((cw[r / 4] >> (8 * (r % 4))) & 0xffu);
+      const int cl = class_of_row(r);
       if constexpr (DO_LIN) row_lin(cl);
       if constexpr (MODE == kAff) row_aff(cl);
-      if constexpr (MODE == kBoth) row_aff(r < 4 ? (int)((cwa0 >> (8 * r)) & 0xffu) : cl);
+      if constexpr (MODE == kBoth) row_aff(r == 0 && pad0 ? kClsPad : cl);
     }
     if (active) {
       cur.pos += R;
@@ -509,8 +533,8 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
             classes(fetch(cur.pos, cur.end), cur.pos, cur.end, true);
           } else {
 #pragma unroll
-            for (int h = 0; h < R / 4; ++h) cw[h] = kPadWord;
-            cwa0 = kPadWord;
+            for (int h = 0; h < NC; ++h) cw[h] = SPREAD ? (uint32_t)kClsPad : kPadWord;
+            pad0 = false;
           }
         }
       } else {
