@@ -56,12 +56,15 @@ constexpr int kMaxQuery = 2048;
 // many rows, and a target's last fetch pads with up to R-1 rows.  Measured
 // (300k targets): affine 8 rows beat 4 by 10% at 27 words per lane, and 16
 // beat 8 by 2-3% at 16 words or fewer but lost 9% at 27 (larger code and
-// register footprint).  Linear 8 rows beat 4 by 3-7% where it fits, but
-// spills under the register caps of many widths, so linear keeps 4, as
-// does the fused kernel (two states in registers).
+// register footprint; with the classes spread over the group's lanes, 16
+// still lost 1-8% at widths 20-32).  Linear 8 rows beat 4 by 4-7% in the
+// narrow layout up to width 13 and the wide one from 17 to 29 (one class
+// register per lane); elsewhere they spill under the register caps, so
+// linear keeps 4 there, as does the fused kernel (two states in registers).
 template <int MODE, int TPT, int W>
 __host__ __device__ constexpr int rows_per_fetch() {
-  return MODE == 1 ? (W * TPT <= 16 ? 16 : 8) : 4;
+  return MODE == 1 ? (W * TPT <= 16 ? 16 : 8)
+       : MODE == 0 && ((W == 1 && TPT <= 13) || (W == 2 && TPT > 16)) ? 8 : 4;
 }
 
 struct SwArgs {
