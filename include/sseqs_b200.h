@@ -104,7 +104,7 @@ int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
  * bytes later) of every target -- identical to the two separate calls
  * (the exact search of sseqs/msa.py:313-332 with top_sw = 1 makes both).
  * Gap parameters must lie in the int16 domain, else SSEQS_ERR_UNSUPPORTED
- * (make the two calls instead).  Queries of up to 512 residues run one
+ * (make the two calls instead).  Queries of up to 672 residues run one
  * fused kernel; longer ones run the two score kernels in turn. */
 int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len, const int32_t* good_idx,
                        int32_t g0, int64_t n_targets, const uint8_t* ascii, const int32_t* delim,

@@ -60,11 +60,14 @@ constexpr int kMaxQuery = 2048;
 // still lost 1-8% at widths 20-32).  Linear 8 rows beat 4 by 4-7% in the
 // narrow layout up to width 13 and the wide one from 17 to 29 (one class
 // register per lane); elsewhere they spill under the register caps, so
-// linear keeps 4 there, as does the fused kernel (two states in registers).
+// linear keeps 4 there.  The fused kernel: 8 rows beat 4 by 1-5% in the
+// narrow layout and lost 16% in the wide one (fewer blocks); they fit the
+// register caps without spilling at widths 9-13 and 18-21 only.
 template <int MODE, int TPT, int W>
 __host__ __device__ constexpr int rows_per_fetch() {
   return MODE == 1 ? (W * TPT <= 16 ? 16 : 8)
-       : MODE == 0 && ((W == 1 && TPT <= 13) || (W == 2 && TPT > 16)) ? 8 : 4;
+       : MODE == 0 && ((W == 1 && TPT <= 13) || (W == 2 && TPT > 16)) ? 8
+       : MODE == 2 && W == 1 && (TPT <= 13 || (TPT >= 18 && TPT <= 21)) ? 8 : 4;
 }
 
 struct SwArgs {
@@ -573,11 +576,11 @@ KernelInfo make_info() {
 // tables[variant][mode][TPT - 1], variant 0 = narrow, 1 = wide;
 // mode kLin, kAff or kBoth.  The fused kernel exists up to kMaxFusedTpt;
 // wider queries run the two kernels one after the other (fn == nullptr
-// here).  Measured on B200 over 1M segments, the fused pass beat the two
-// kernels by 4-17% up to 16 words per lane but lost 4% at 22-27 and 13% at
-// 41-48: its three states need ~200-255 registers there, which leaves 8
-// warps per SM instead of 16.
-constexpr int kMaxFusedTpt = 16;
+// here).  Measured on B200 (300k-1M segments), the fused pass beat the two
+// kernels by 4-17% up to width 16 and by 5% at 20 (8 rows per fetch),
+// broke even at 27 and lost 13% at 41-48: its three states need ~200-255
+// registers there, which leaves 8 warps per SM.
+constexpr int kMaxFusedTpt = 21;
 struct Tables {
   KernelInfo k[2][3][64];
 };

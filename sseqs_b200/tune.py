@@ -26,7 +26,7 @@ def tpt_of(query_len: int) -> int:
 
 
 MODES = ("linear", "affine", "both")
-MAX_FUSED_TPT = 16      # widths scored by the fused pass (wider: the two kernels)
+MAX_FUSED_TPT = 21      # widths scored by the fused pass (wider: the two kernels)
 
 
 def set_variant(affine, tpt: int, wide: int) -> None:

@@ -169,7 +169,7 @@ def _set_variant(mode, tpt, wide):
     _lib.check(_lib.lib().sseqs_sw_set_variant(mode, tpt, wide), "set_variant")
 
 
-@pytest.mark.parametrize("Lq", [1, 20, 33, 64, 100, 200, 287, 500, 545, 858, 1000, 1300, 1536,
+@pytest.mark.parametrize("Lq", [1, 20, 33, 64, 100, 200, 287, 500, 545, 640, 672, 673, 858, 1000, 1300, 1536,
                                 1537, 2048])
 @pytest.mark.parametrize("wide", [0, 1])
 def test_scan_both_equals_two_scans(Lq, wide):
