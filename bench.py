@@ -144,13 +144,13 @@ def run_step(M, query, db, timer=None, world=1, rank=0):
     """Device part of one step: search, rank, traceback (no file I/O).  With
     several GPUs every rank searches its own shard, the ranked hits are merged
     across ranks, and rank 0 aligns the merged list."""
-    from sseqs_b200.to_a3m import align_all
+    from sseqs_b200.to_a3m import traceback_all
     rows = M.search([query], db, num_msas=TOP_K, top_fft=1, top_sw=1, top_sw_affine=TOP_K,
                     timer=timer)[0]
     if world > 1:
         from sseqs_b200 import shard
         rows = [r[:1] + r[2:] for r in shard.gather_hits(rows, TOP_K)]
-    al = align_all(query, [r[5] for r in rows]) if rank == 0 else None
+    al = traceback_all(query, [r[5] for r in rows]) if rank == 0 else None
     return rows, al
 
 
@@ -160,7 +160,7 @@ def prefiltered_leg(M, db, queries, exact_rows, per_query=32768):
     linear + affine SW of the candidates, top-4096, traceback.  Reports
     queries/s and recall of the exact search's top-1000 hits."""
     import torch
-    from sseqs_b200.to_a3m import align_all
+    from sseqs_b200.to_a3m import traceback_all
     nb = len(db.batches)
     seg_per_batch = max(b.n_segments for b in db.batches)
     top_fft = max(1, seg_per_batch // max(1, per_query // nb))
@@ -174,7 +174,7 @@ def prefiltered_leg(M, db, queries, exact_rows, per_query=32768):
     for q in queries:
         rows = M.search([q], db, num_msas=TOP_K, top_fft=top_fft, top_sw=1,
                         top_sw_affine=TOP_K)[0]
-        align_all(q, [r[5] for r in rows])
+        traceback_all(q, [r[5] for r in rows])
         results.append(rows)
     e1.record()
     torch.cuda.synchronize()
@@ -314,7 +314,7 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
     recall of the exact search's top-1000 over the exact leg's queries."""
     import torch
     from sseqs_b200 import dbtools, learned
-    from sseqs_b200.to_a3m import align_all
+    from sseqs_b200.to_a3m import traceback_all
     per_query = 256
     t0 = time.time()
     pairs = learned.training_pairs(max(1, n_pairs // per_query), per_query, seed=seed)
@@ -335,7 +335,7 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
     def step(batch_q):
         res = index.search(batch_q, n_cand=32768, top=TOP_K)
         for q, rows in zip(batch_q, res):
-            align_all(q, learned.hit_strings(db, rows))
+            traceback_all(q, learned.hit_strings(db, rows))
         return res
 
     step(qs[:2])

@@ -213,6 +213,25 @@ int sseqs_backtrack_affine(const uint8_t* query, int query_len, const uint8_t* t
                            uint8_t* q_aligned, uint8_t* t_aligned, int cap, int32_t* m_full,
                            int tcols, void* workspace, size_t ws_bytes, cudaStream_t stream);
 
+/* a3m rows of traceback results (host function; every pointer is host
+ * memory).  Row k is the alignment q_rows[k][0..lens[k]) / t_rows[k][..)
+ * (ASCII bytes, '-' for gaps) with integer score scores[k]; rows are taken
+ * in order[0..n_rows) (the caller's descending sort of the scores).  Each
+ * kept row is written as ">target_<i> score=<score>.0\n<row>\n" where i is
+ * its position in `order` and <row> places the alignment at the first
+ * occurrence of its gap-free query fragment in `query`, padded with '-' to
+ * the query's length, target residues upper case against a query residue
+ * and lower case against a query gap.  Rows with score 0 or no alignment,
+ * rows holding '@' and repeats of an earlier row are skipped.  Replaces the
+ * row loop of to_a3m (sseqs/to_a3m.py:16-72).  *out_len receives the bytes
+ * written to out; SSEQS_ERR_UNSUPPORTED when a fragment does not occur in
+ * the query (the reference raises ValueError), SSEQS_ERR_CAPACITY when
+ * out_cap is too small. */
+int sseqs_a3m_rows(const char* query, int64_t query_len, int64_t n_rows, const int64_t* order,
+                   const uint8_t* const* q_rows, const uint8_t* const* t_rows,
+                   const int32_t* lens, const int64_t* scores, char* out, int64_t out_cap,
+                   int64_t* out_len);
+
 /* ------------------------------------------------------------ prefilter */
 /* Gapless rank-k correlation score of every segment (fp16 out[s]):
  * 0.5 * max over even lags of sum_r (a_r (*) b_r), a cyclic convolution of

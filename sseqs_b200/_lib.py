@@ -47,6 +47,7 @@ _SIGNATURES = {
     "sseqs_backtrack_workspace_bytes": (_SZ, [_I, _I, _I]),
     "sseqs_backtrack_affine": (_I, [_P, _I, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I,
                                     _P, _I, _P, _SZ, _P]),
+    "sseqs_a3m_rows": (_I, [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _I64, _P]),
     "sseqs_prefilter_workspace_bytes": (_SZ, [_I, _I]),
     "sseqs_prefilter": (_I, [_P, _P, _P, _I64, _P, _I, _P, _P, _I, _I, _P, _P, _SZ, _P]),
     "sseqs_dpx_peak": (_I, [_P, ctypes.POINTER(_D), _P]),

@@ -144,19 +144,40 @@ def _norm(aff: np.ndarray, Lq: int, maxlen: int) -> np.ndarray:
 
 def rank_hits(query: str, per_batch: list, num_msas: int):
     """Concatenate batch hits, order by normalised score (desc), then batch
-    and segment position (asc); keep ``num_msas`` (msa.py:411-427)."""
-    rows = []
-    for bh in per_batch:
-        if bh is None:
-            continue
+    and segment position (asc); keep ``num_msas`` (msa.py:411-427).
+
+    The order is one stable ``np.lexsort`` on those keys (segments are
+    unique within a batch, so it is the order of the reference's sort), and
+    only the kept rows' hit bytes are gathered and decoded.
+    """
+    parts = [bh for bh in per_batch if bh is not None and bh.g.numel() > 0]
+    if not parts:
+        return []
+    cols = {k: [] for k in ("norm", "batch", "g", "aff", "lin", "part", "row")}
+    for j, bh in enumerate(parts):
         g, aff, lin = to_host(bh.g), to_host(bh.affine), to_host(bh.linear)
-        hb, hl = to_host(bh.hits), to_host(bh.hit_len)
-        norm = _norm(aff, len(query), bh.maxlen)
-        for r in range(g.size):
-            rows.append((float(norm[r]), bh.batch, int(g[r]), int(aff[r]), int(lin[r]),
-                         hb[r, :hl[r]].tobytes().decode("latin-1")))
-    rows.sort(key=lambda x: (-x[0], x[1], x[2]))
-    return rows[:num_msas]
+        cols["norm"].append(_norm(aff, len(query), bh.maxlen))
+        cols["batch"].append(np.full(g.size, bh.batch, dtype=np.int64))
+        cols["g"].append(g.astype(np.int64))
+        cols["aff"].append(aff)
+        cols["lin"].append(lin)
+        cols["part"].append(np.full(g.size, j, dtype=np.int64))
+        cols["row"].append(np.arange(g.size, dtype=np.int64))
+    c = {k: np.concatenate(v) for k, v in cols.items()}
+    keep = np.lexsort((c["g"], c["batch"], -c["norm"].astype(np.float64)))[:num_msas]
+    kpart, krow = c["part"][keep], c["row"][keep]
+    hits = [None] * keep.size
+    for j, bh in enumerate(parts):
+        pos = np.flatnonzero(kpart == j)
+        if pos.size == 0:
+            continue
+        idx = torch.from_numpy(krow[pos]).to(bh.hits.device)
+        hb, hl = to_host(bh.hits.index_select(0, idx)), to_host(bh.hit_len.index_select(0, idx))
+        blob, w = hb.tobytes(), hb.shape[1]
+        for r, (p, n) in enumerate(zip(pos.tolist(), hl.tolist())):
+            hits[p] = blob[r * w:r * w + min(max(n, 0), w)].decode("latin-1")
+    return list(zip(c["norm"][keep].tolist(), c["batch"][keep].tolist(), c["g"][keep].tolist(),
+                    c["aff"][keep].tolist(), c["lin"][keep].tolist(), hits))
 
 
 def search(queries, db: Database | None = None, *, num_msas=4096, top_fft=200, top_sw=10,
