@@ -180,15 +180,20 @@ constexpr int kLin = 0, kAff = 1, kBoth = 2;
 // share one copy of the query profile in shared memory, with the register
 // cap set for 3 blocks (85 registers) or 2 (128) per SM; larger states use
 // blocks of 4 warps, which pack the register file more finely (the fused
-// kernel capped for 3 of them, 170 registers, when its estimate allows).
+// kernel and the wide linear layout capped for 3 of them, 170 registers,
+// when the estimate allows).  The affine kernel at 17 words per lane (8
+// rows per fetch) ran 7% slower under the 85-register cap than with 128, so
+// the 3-block cap is not used where affine fetches 8 rows.
 template <int TPT, int W, int MODE>
 struct Shape {
   static constexpr int NWD = W * TPT;
   static constexpr int est_regs = MODE == kAff ? 3 * NWD + 32
                                 : MODE == kLin ? 2 * NWD + 53 : 5 * NWD + 40;
+  static constexpr bool cap85 =
+      est_regs <= 85 && !(MODE == kAff && rows_per_fetch<MODE, TPT, W>() == 8);
   static constexpr int threads = est_regs <= 128 ? 256 : 128;
   static constexpr int min_blocks =
-      threads == 256 ? (est_regs <= 85 ? 3 : 2)
+      threads == 256 ? (cap85 ? 3 : 2)
                      : ((MODE == kBoth || (MODE == kLin && TPT > 16 && W == 2)) &&
                         est_regs <= 170 ? 3 : 1);
 };
