@@ -71,6 +71,7 @@ class Database:
         self.batches: list[Batch] = []
         self.packed = [] if keep_packed else None
         self.n_residues = 0
+        self.index = None          # sidecar segment index (from_file), if any
         for ci, ch in enumerate(chunks):
             ch = ch if isinstance(ch, torch.Tensor) else torch.from_numpy(np.asarray(ch, np.uint8))
             ch = ch.to(self.device, torch.uint8)
@@ -103,7 +104,10 @@ class Database:
     def from_file(cls, path: str, chunks: int | None = None, bs: int = CHUNK_BYTES,
                   device="cuda", chunk_bytes: int = CHUNK_BYTES):
         """Read ``chunks`` chunks of ``chunk_bytes`` from an .xbit file
-        (sseqs/msa.py:50-55); bytes past the end of the file read as 0."""
+        (sseqs/msa.py:50-55); bytes past the end of the file read as 0.  A
+        sidecar segment index next to the file (``dbtools.fasta_to_xbit``)
+        is loaded as ``index`` when its chunk size matches."""
+        from .dbtools import SeqIndex, index_path
         size = os.path.getsize(path)
         n = math.ceil(size / chunk_bytes) if chunks is None else int(chunks)
         out = []
@@ -113,7 +117,36 @@ class Database:
                 fh.seek(i * chunk_bytes)
                 fh.readinto(memoryview(buf))
                 out.append(torch.from_numpy(buf))
-        return cls(out, bs=bs, device=device)
+        db = cls(out, bs=bs, device=device)
+        if os.path.exists(index_path(path)):
+            idx = SeqIndex.load(index_path(path))
+            if idx.chunk_bytes == chunk_bytes:
+                db.index = idx
+        return db
+
+    def hit_names(self, hits) -> list:
+        """FASTA names of ranked hits ((…, batch, segment, …) rows as
+        ``msa.search`` returns them): the sequence holding the first byte of
+        the hit's window (``offsets[g]`` of its batch, the bytes the hit
+        string shows), from the sidecar index; None where a position is not
+        inside a sequence."""
+        if self.index is None:
+            raise ValueError("no sidecar segment index loaded for this database")
+        if (self.bs * 8) % 5:
+            raise ValueError("batch boundaries fall inside a 5-byte group (bs % 5 != 0)")
+        by_batch: dict = {}
+        for r, row in enumerate(hits):
+            by_batch.setdefault(int(row[1]), []).append((r, int(row[2])))
+        names = [None] * len(hits)
+        for bi, items in by_batch.items():
+            b = self.batches[bi]
+            g = torch.tensor([x[1] for x in items], dtype=torch.int64, device=b.offsets.device)
+            off = b.offsets.index_select(0, g).cpu().numpy()
+            base = b.index * self.bs * 8 // 5
+            for (r, _), o in zip(items, off.tolist()):
+                k = self.index.locate(b.chunk, base + o)
+                names[r] = self.index.names[k] if k >= 0 else None
+        return names
 
     @property
     def n_segments(self) -> int:

@@ -1,4 +1,5 @@
-"""Database tooling: the .xbit packer and a seeded synthetic database generator.
+"""Database tooling: the .xbit packer (from sequences or a FASTA file, with a
+sidecar segment index) and a seeded synthetic database generator.
 
 File layout (as read by sseqs/msa.py:50-55 and decoded by sseqs/xbit.cu:8-34):
 a raw, header-less 5-bit stream of ``S0@S1@...@`` in chunks of ``chunk_bytes``
@@ -232,3 +233,121 @@ def write_xbit(path: str, sequences, chunk_bytes: int = CHUNK_BYTES) -> int:
         for c in chunks:
             f.write(c.cpu().numpy().tobytes())
     return len(chunks)
+
+
+# --------------------------------------------------------- FASTA -> .xbit
+def read_fasta(path: str):
+    """(name, sequence) of every record of a FASTA file: the name is the
+    header line after '>' (stripped), the sequence its following lines with
+    whitespace removed; text before the first header is ignored."""
+    name, parts = None, []
+    with open(path, "r", encoding="latin-1") as fh:
+        for line in fh:
+            if line.startswith(">"):
+                if name is not None:
+                    yield name, "".join(parts)
+                name, parts = line[1:].strip(), []
+            elif name is not None:
+                parts.append("".join(line.split()))
+    if name is not None:
+        yield name, "".join(parts)
+
+
+_RESIDUE_MAP = np.full(256, ord("X"), np.uint8)
+_RESIDUE_MAP[ord("A"):ord("Z") + 1] = np.arange(ord("A"), ord("Z") + 1)
+_RESIDUE_MAP[ord("a"):ord("z") + 1] = np.arange(ord("A"), ord("Z") + 1)
+
+
+def normalise_residues(seq: str) -> bytes:
+    """The bytes a sequence is stored as: letters upper-cased, every other
+    character 'X'.  (The 5-bit alphabet holds '@'..'_'; the reference's
+    packer, sseqs/xbit.cu:47-49, keeps the low 5 bits of byte - 64, which
+    would turn '*' into 'J' and '-' into 'M'.)"""
+    return _RESIDUE_MAP[np.frombuffer(seq.encode("latin-1"), np.uint8)].tobytes()
+
+
+@dataclass
+class SeqIndex:
+    """Sidecar segment index of an .xbit file: for sequence k (file order),
+    its chunk, its first symbol inside that chunk, its length and its name."""
+    chunk_bytes: int
+    n_chunks: int
+    chunk_of: np.ndarray       # int32[n]
+    start: np.ndarray          # int64[n] symbol position inside the chunk
+    length: np.ndarray         # int32[n]
+    names: list
+
+    def save(self, path: str) -> None:
+        blob = "\n".join(self.names).encode("latin-1") if self.names else b""
+        with open(path, "wb") as fh:
+            np.savez(fh, chunk_bytes=np.int64(self.chunk_bytes), n_chunks=np.int64(self.n_chunks),
+                     chunk_of=self.chunk_of, start=self.start, length=self.length,
+                     names=np.frombuffer(blob, np.uint8), n=np.int64(len(self.names)))
+
+    @classmethod
+    def load(cls, path: str) -> "SeqIndex":
+        z = np.load(path)
+        n = int(z["n"])
+        names = z["names"].tobytes().decode("latin-1").split("\n") if n else []
+        return cls(int(z["chunk_bytes"]), int(z["n_chunks"]), z["chunk_of"], z["start"],
+                   z["length"], names)
+
+    def locate(self, chunk: int, pos: int) -> int:
+        """Sequence whose bytes or closing '@' hold symbol ``pos`` of
+        ``chunk`` (-1 for chunk padding)."""
+        lo = int(np.searchsorted(self.chunk_of, chunk, side="left"))
+        hi = int(np.searchsorted(self.chunk_of, chunk, side="right"))
+        if lo == hi:
+            return -1
+        k = lo + int(np.searchsorted(self.start[lo:hi], pos, side="right")) - 1
+        if k < lo or pos > self.start[k] + self.length[k]:
+            return -1
+        return k
+
+
+def index_path(xbit_path: str) -> str:
+    """Where the sidecar index of an .xbit file lives."""
+    return xbit_path + ".idx.npz"
+
+
+def fasta_to_xbit(fasta_path: str, xbit_path: str, chunk_bytes: int = CHUNK_BYTES,
+                  sidecar: str | None = None) -> SeqIndex:
+    """Pack a FASTA file into a chunk-aligned .xbit file (the layout
+    ``write_xbit`` writes, byte for byte, for the normalised sequences) and
+    write its sidecar segment index (``index_path(xbit_path)`` unless given).
+
+    Streams the input: one chunk of symbols is held at a time.  A sequence
+    longer than a chunk raises ValueError."""
+    cap = chunk_bytes * 8 // 5                       # symbols per chunk
+    chunk_of, start, length, names = [], [], [], []
+    buf = np.full(cap, 64, np.uint8)
+    used, ci = 0, 0
+
+    def flush(fh):
+        packed = pack_symbols_host(buf)
+        fh.write(packed.tobytes())
+        if packed.size < chunk_bytes:
+            fh.write(bytes(chunk_bytes - packed.size))
+
+    with open(xbit_path, "wb") as fh:
+        for name, seq in read_fasta(fasta_path):
+            s = np.frombuffer(normalise_residues(seq), np.uint8)
+            if s.size + 1 > cap:
+                raise ValueError(f"sequence {name!r} ({s.size} residues) is longer than a chunk")
+            if used + s.size + 1 > cap:
+                flush(fh)
+                buf[:] = 64
+                used, ci = 0, ci + 1
+            buf[used:used + s.size] = s
+            chunk_of.append(ci)
+            start.append(used)
+            length.append(s.size)
+            names.append(name.replace("\n", " "))
+            used += s.size + 1
+        if used:
+            flush(fh)
+            ci += 1
+    idx = SeqIndex(chunk_bytes, ci, np.asarray(chunk_of, np.int32), np.asarray(start, np.int64),
+                   np.asarray(length, np.int32), names)
+    idx.save(sidecar or index_path(xbit_path))
+    return idx

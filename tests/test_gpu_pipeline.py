@@ -130,3 +130,42 @@ def test_msa_writes_oracle_a3m(tmp_path):
     assert f.read_text() == O.to_a3m_text(q, al)
     # planted homologs dominate the top of the list
     assert sum(1 for r in rows[:20] if r[3] > 100) >= 15
+
+
+def test_fasta_database_names_its_hits(tmp_path):
+    """A FASTA file packed with its sidecar index, loaded with batches smaller
+    than a chunk: every ranked hit's string lies inside the sequence its
+    name (from the index) points at, and planted homologs are named."""
+    from sseqs_b200 import dbtools
+    from sseqs_b200.database import Database
+    M = importlib.import_module("sseqs_b200.msa")
+    rng = np.random.default_rng(9)
+    q = dbtools.random_query(150, 9)
+    seqs = {}
+    lines = []
+    for i in range(1500):
+        if i % 97 == 0:        # planted homolog: a mutated copy of the query
+            s = "".join(c if rng.random() < 0.8 else "ACDEFGHIKLMNPQRSTVWY"[rng.integers(20)]
+                        for c in q)
+            name = f"hom{i} planted"
+        else:
+            s = dbtools.random_query(int(rng.integers(20, 400)), 5000 + i)
+            name = f"bg{i}"
+        seqs[name] = s
+        lines.append(f">{name}\n{s[:60]}\n{s[60:]}\n")
+    fa = tmp_path / "db.fasta"
+    fa.write_text("".join(lines))
+    xb = str(tmp_path / "db.xbit")
+    idx = dbtools.fasta_to_xbit(str(fa), xb, chunk_bytes=100_000)
+    assert idx.n_chunks >= 3
+    db = Database.from_file(xb, bs=50_000, chunk_bytes=100_000)
+    assert db.index is not None
+    rows = M.search([q], db, num_msas=300, top_fft=1, top_sw=1, top_sw_affine=300)[0]
+    names = db.hit_names(rows)
+    assert len(names) == len(rows)
+    for row, name in zip(rows, names):
+        assert name is not None and row[5] in seqs[name], (row[1], row[2], name)
+    # 16 planted; the first and last segment of every batch are not searched
+    # (sseqs/msa.py:307), which can take out a few
+    planted = [n for n in names[:16] if n.startswith("hom")]
+    assert len(planted) >= 12
