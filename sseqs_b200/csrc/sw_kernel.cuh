@@ -167,6 +167,17 @@ struct Layout {
   static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
 };
 
+// The linear recurrence issues 2 int16x2 adds per word on the FMA pipe
+// (both half rate) and 1.5 maxima on the ALU pipe, so its FMA pipe is the
+// busier one (ncu at width 27: 2.4 FMA against 1.9 ALU instructions per
+// word).  Every kLinAluEvery-th column takes the add onto the ALU pipe
+// (one add-max instead of add + max); measured on B200 (300k targets, same
+// scores) every 4th column was 0.3-3% faster at widths 13-32 and 2% slower
+// at width 5 (every 2nd or 3rd: mixed, -3% to +1%), so it applies from
+// width 9 -- except 17-18, where it made the wide layout spill.
+template <int TPT>
+constexpr int lin_alu_every() { return TPT >= 9 && (TPT < 17 || TPT > 18) ? 4 : 0; }
+
 // Score variants of one instantiation: the linear kernel, the affine kernel,
 // or both in one pass over the targets (the exact search scores every
 // target with both; one pass shares the byte fetch, the per-row loads and
@@ -325,9 +336,17 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       for (int k = 0; k < TPT; ++k) {
         const uint32_t up = SL[w][k];
         const uint32_t u_next = (k + 1 < TPT) ? __vadd2(up, s[w * TPT + k + 1]) : 0u;
-        const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
-                                    : __vimax3_s16x2_relu(u, up, hg_left);   // ALU pipe
-        hg_left = __vadd2(h, gap2);                                         // FMA pipe
+        constexpr int EV = lin_alu_every<TPT>();
+        if (MODE == kLin && EV > 0 && k % (EV > 0 ? EV : 1) == EV - 1) {
+          // the same value with the add on the ALU pipe:
+          // max(m + gap, gap) = max(m, 0) + gap, m >= Hg_up >= gap >= -16384
+          const uint32_t m = (k == 0) ? __vmaxs2(u, up) : __vimax3_s16x2(u, up, hg_left);
+          hg_left = __viaddmax_s16x2(m, gap2, gap2);                        // ALU pipe
+        } else {
+          const uint32_t h = (k == 0) ? __vimax_s16x2_relu(u, up)
+                                      : __vimax3_s16x2_relu(u, up, hg_left); // ALU pipe
+          hg_left = __vadd2(h, gap2);                                       // FMA pipe
+        }
         SL[w][k] = hg_left;
         if (((w * TPT + k) & 1) == 0) pend = u;
         else bestL = __vimax3_s16x2(bestL, pend, u);
