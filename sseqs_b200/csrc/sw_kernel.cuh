@@ -156,14 +156,29 @@ constexpr int words_for() {
   return TPT == 1 ? 16 : TPT == 2 ? 8 : TPT <= 4 ? 4 : TPT <= 8 ? 2 : 1;
 }
 
-template <int TPT, int W>
+// Profile layout of one residue class.  Lane-major: lane gl's NV 16-byte
+// vectors are contiguous, padded to an odd count so that the 8 lanes of a
+// quarter warp hit distinct banks.  Vector-major (VM): vector v of lane gl
+// at slot v * G + gl, so those 8 lanes read 8 consecutive slots (all 32
+// banks once) with no padding -- up to 25% less shared memory, which gave
+// the fused kernel a third block per SM at widths 21-24 (3.5-6.6% faster)
+// and the wide linear layout at 27 2.6% faster; with fewer than 16 lanes
+// per target it was 1-3% slower elsewhere (the quarter warp then spans
+// groups reading different classes), so those keep the lane-major layout
+// (the wide linear layout takes VM from width 19).
+template <int TPT, int W, int MODE>
+constexpr bool vector_major() { return W == 1 || (MODE == 0 && W == 2 && TPT > 18); }
+
+template <int TPT, int W, bool VM>
 struct Layout {
   static constexpr int G = 32 / (2 * W);    // lanes per target
   static constexpr int GPW = 2 * W;         // targets per warp
   static constexpr int NWD = W * TPT;       // profile words per lane and row
   static constexpr int NV = (NWD + 3) / 4;  // 128-bit loads per lane and row
-  static constexpr int LWP = ((NV % 2) ? NV : NV + 1) * 4;  // odd # of uint4
+  static constexpr int LWP = VM ? NV * 4 : ((NV % 2) ? NV : NV + 1) * 4;  // words per lane
   static constexpr int CLS = G * LWP;       // words per residue class
+  static constexpr int LANE_STEP = VM ? 1 : LWP / 4;   // uint4 slots from lane to lane
+  static constexpr int VEC_STEP = VM ? G : 1;          // uint4 slots from vector to vector
   static constexpr size_t smem = (size_t)kNumCls * CLS * 4 + 256;
 };
 
@@ -212,7 +227,8 @@ struct Shape {
 template <int TPT, int W, int MODE>
 __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MODE>::min_blocks)
     sw_stream_kernel(SwArgs a, const QueryTable qt) {
-  using L = Layout<TPT, W>;
+  constexpr bool VM = vector_major<TPT, W, MODE>();
+  using L = Layout<TPT, W, VM>;
   constexpr bool DO_LIN = MODE != kAff, DO_AFF = MODE != kLin;
   constexpr int NTAB = MODE == kBoth ? 2 : 1;
   if (qt.n > 0) {
@@ -253,7 +269,9 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
     const bool aff_tab = MODE == kAff || tb == 1;
     const int pad = aff_tab ? kNeg + open : -16384;
     const int c = ii / L::CLS, r = ii - c * L::CLS;
-    const int gl = r / L::LWP, v = r - gl * L::LWP;
+    const int slot = r >> 2;                          // uint4 slot in the class
+    const int gl = VM ? slot % G : slot / L::LANE_STEP;
+    const int v = (VM ? slot / G : slot % L::LANE_STEP) * 4 + (r & 3);   // word of lane gl
     uint32_t word = pack2(pad, pad);
     if (v < L::NWD) {
       const int w = v / TPT, k = v - w * TPT;
@@ -300,11 +318,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
 
   // one linear DP row for every group of the warp (warp-uniform)
   auto row_lin = [&](int cls) {
-    const uint4* pr = reinterpret_cast<const uint4*>(profL + cls * L::CLS + gl * L::LWP);
+    const uint4* pr = reinterpret_cast<const uint4*>(profL + cls * L::CLS) + gl * L::LANE_STEP;
     uint32_t s[L::NV * 4];
 #pragma unroll
     for (int v = 0; v < L::NV; ++v) {
-      const uint4 x = pr[v];
+      const uint4 x = pr[v * L::VEC_STEP];
       s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
     uint32_t from_left = __shfl_up_sync(0xffffffffu, SL[WL - 1][TPT - 1], 1, G);
@@ -358,11 +376,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
 
   // one affine DP row for every group of the warp (warp-uniform)
   auto row_aff = [&](int cls) {
-    const uint4* pr = reinterpret_cast<const uint4*>(profA + cls * L::CLS + gl * L::LWP);
+    const uint4* pr = reinterpret_cast<const uint4*>(profA + cls * L::CLS) + gl * L::LANE_STEP;
     uint32_t s[L::NV * 4];
 #pragma unroll
     for (int v = 0; v < L::NV; ++v) {
-      const uint4 x = pr[v];
+      const uint4 x = pr[v * L::VEC_STEP];
       s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
     uint32_t from_left = __shfl_up_sync(0xffffffffu, SA[WA - 1][TPT - 1], 1, G);
@@ -590,9 +608,10 @@ KernelInfo make_info() {
   constexpr int W = words_for<TPT, WIDE, MODE>();
   KernelInfo k;
   k.fn = sw_stream_kernel<TPT, W, MODE>;
-  k.smem = Layout<TPT, W>::smem + (MODE == kBoth ? Layout<TPT, W>::smem - 256 : 0);
+  using L = Layout<TPT, W, vector_major<TPT, W, MODE>()>;
+  k.smem = L::smem + (MODE == kBoth ? L::smem - 256 : 0);
   k.threads = Shape<TPT, W, MODE>::threads;
-  k.groups_per_block = (k.threads / 32) * Layout<TPT, W>::GPW;
+  k.groups_per_block = (k.threads / 32) * L::GPW;
   k.words = W;
   return k;
 }
