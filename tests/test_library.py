@@ -69,3 +69,50 @@ def test_batched_buckets_group_by_stripe_width():
     assert b == {10: [6, 0], 1: [7, 1, 2], 2: [3, 5], 64: [4]}
     for tpt, members in b.items():
         assert all((lengths[i] + 31) // 32 == tpt for i in members)
+
+
+def test_score_kernel_registry_matches_dispatch_rules(built_lib):
+    """The instantiated score kernels are the ones the host dispatch counts
+    on: the fused pass up to width 21 (``tune.fused``), a wide layout of its
+    own for the linear kernel at widths 2-29 and for the affine and fused
+    kernels at 2-16 (``tune.has_wide``; at width 1 both layouts hold 16
+    words per lane).  Read from the library's registry;
+    no GPU needed."""
+    from sseqs_b200 import _lib, tune
+    L = _lib.lib()
+    words = lambda mode, t, wide: L.sseqs_sw_variant_words(mode, t, wide)
+    assert tune.MAX_FUSED_TPT == 21
+    for t in range(1, 65):
+        assert (words(2, t, 0) > 0) == (t <= 21), t
+        assert tune.fused(32 * t) == (t <= 21)
+        assert words(0, t, 0) > 0 and words(1, t, 0) > 0
+        assert tune.has_wide(0, t) == (2 <= t <= 29), t
+        assert tune.has_wide(1, t) == (2 <= t <= 16), t
+        if t <= 21:
+            assert tune.has_wide(2, t) == (2 <= t <= 16), t
+    assert words(0, 27, 1) == 2 and words(0, 27, 0) == 1
+    assert L.sseqs_sw_variant_words(3, 5, 0) == -1 and L.sseqs_sw_variant_words(0, 65, 0) == -1
+
+
+def test_scan_both_argument_checks_without_a_gpu(built_lib):
+    """sseqs_sw_scan_both rejects bad arguments on the host, before any
+    CUDA call: a window shift other than 0/1, a missing output, a query
+    outside 1..2048, gaps outside the int16 domain; no targets is a no-op."""
+    import ctypes
+    from sseqs_b200 import _lib
+    L = _lib.lib()
+    fake = ctypes.c_void_p(16)              # never dereferenced: every call returns early
+    assert L.sseqs_sw_scan_both(fake, 10, None, 0, 0, fake, fake, 1, fake, fake, -1, 11, 1,
+                                None) == 0
+    assert L.sseqs_sw_scan_both(fake, 10, None, 0, 5, fake, fake, 2, fake, fake, -1, 11, 1,
+                                None) == 1
+    assert L.sseqs_sw_scan_both(fake, 10, None, 0, 5, fake, fake, 1, None, fake, -1, 11, 1,
+                                None) == 1
+    assert L.sseqs_sw_scan_both(fake, 0, None, 0, 5, fake, fake, 1, fake, fake, -1, 11, 1,
+                                None) == 1
+    assert L.sseqs_sw_scan_both(fake, 2049, None, 0, 5, fake, fake, 1, fake, fake, -1, 11, 1,
+                                None) == 2
+    assert L.sseqs_sw_scan_both(fake, 10, None, 0, 5, fake, fake, 1, fake, fake, 1, 11, 1,
+                                None) == 2
+    assert L.sseqs_sw_scan_both(fake, 10, None, 0, 5, fake, fake, 1, fake, fake, -1, -3, 1,
+                                None) == 2
