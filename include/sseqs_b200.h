@@ -102,10 +102,17 @@ int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
  * score (gap, windows as sseqs_sw_scan with skip 0) and out_affine[t] the
  * affine score (gap_open, gap_extend, windows starting affine_skip (0 or 1)
  * bytes later) of every target -- identical to the two separate calls
- * (the exact search of sseqs/msa.py:313-332 with top_sw = 1 makes both).
+ * (the exact search of sseqs/msa.py:313-332 with top_sw = 1 makes both),
+ * including query_len 0, where every result of both is -1.
  * Gap parameters must lie in the int16 domain, else SSEQS_ERR_UNSUPPORTED
  * (make the two calls instead).  Queries of up to 672 residues run one
- * fused kernel; longer ones run the two score kernels in turn. */
+ * fused kernel; longer ones run the two score kernels in turn.
+ * Like every single-query scan, it takes its target counter from a ring of
+ * 1024 library-owned slots, one per launch: eager calls overlapping on
+ * other streams never share one, but a call captured into a CUDA graph
+ * keeps its slot for every replay, so a replay must not overlap other
+ * single-query scans (the batched call below takes caller-owned counters
+ * and has no such limit). */
 int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len, const int32_t* good_idx,
                        int32_t g0, int64_t n_targets, const uint8_t* ascii, const int32_t* delim,
                        int affine_skip, int32_t* out_linear, int32_t* out_affine, int gap,
@@ -269,6 +276,9 @@ int64_t sseqs_launch_count(void);
  * used for (affine, tpt); both give identical scores.  No reference
  * counterpart (the autotuner of the batched path sets it). */
 int sseqs_sw_set_variant(int affine, int tpt, int wide);
+/* The layout currently selected for (affine, tpt): 0 or 1; -1 if out of
+ * range.  No reference counterpart. */
+int sseqs_sw_get_variant(int affine, int tpt);
 /* int16x2 words per lane of a variant (for reports); -1 if out of range. */
 int sseqs_sw_variant_words(int affine, int tpt, int wide);
 

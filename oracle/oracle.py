@@ -257,9 +257,16 @@ def prefilter_scores(query: str, A, B, ascii, offsets, lengths, n, k=4):
     alphabet) reads the next rank's entry 0 (fft.cu:91,124); for the last
     rank that read is past the table and is taken as 0 here.
     """
-    k = max(1, min(k, A.shape[0]))
     qrev = np.array([AA_TO_POS.get(c, 20) for c in query[::-1]], np.int64)
-    Lq = len(query)
+    return prefilter_scores_codes(qrev, A, B, ascii, offsets, lengths, n, k)
+
+
+def prefilter_scores_codes(qrev, A, B, ascii, offsets, lengths, n, k=4):
+    """``prefilter_scores`` given the reversed query as 0..20 codes, the form
+    ``warp_corr`` receives it in (sseqs/msa.py:157, filter_bind.cpp:20-64)."""
+    k = max(1, min(k, A.shape[0]))
+    qrev = np.asarray(qrev, np.int64)
+    Lq = qrev.size
     a = np.zeros((k, n))
     a[:, :Lq] = A[:k][:, qrev]
     Bx = np.zeros((k, 22))

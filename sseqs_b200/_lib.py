@@ -72,6 +72,7 @@ _SIGNATURES = {
     "sseqs_score_dense": (_I, [_P, _I, _P, _I64, _P, _P]),
     "sseqs_kth_largest_rows": (_I, [_P, _I, _I, _I, _P, _P]),
     "sseqs_sw_variant_words": (_I, [_I, _I, _I]),
+    "sseqs_sw_get_variant": (_I, [_I, _I]),
 }
 
 _lock = threading.Lock()

@@ -306,9 +306,16 @@ extern "C" int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len,
                                   int gap_open, int gap_extend, cudaStream_t stream) {
   if (g0 < 0 || n_targets < 0 || (affine_skip != 0 && affine_skip != 1)) return SSEQS_ERR_ARG;
   if (n_targets == 0) return SSEQS_OK;
-  if (!out_linear || !out_affine || !delim || !ascii || !query_idx) return SSEQS_ERR_ARG;
-  if (query_len < 1) return SSEQS_ERR_ARG;
+  if (!out_linear || !out_affine || !delim || !ascii) return SSEQS_ERR_ARG;
+  if (query_len < 0) return SSEQS_ERR_ARG;
   if (query_len > kMaxQuery) return SSEQS_ERR_UNSUPPORTED;
+  if (query_len == 0) {   // as the two scans: every result -1 (sseqs/sw.cu:73, :201)
+    const int grid = (int)std::min<int64_t>((n_targets + 255) / 256, 4096);
+    { fill_kernel<<<grid, 256, 0, stream>>>(out_linear, n_targets, -1); count_launches(1); }
+    { fill_kernel<<<grid, 256, 0, stream>>>(out_affine, n_targets, -1); count_launches(1); }
+    return status_of(cudaGetLastError());
+  }
+  if (!query_idx) return SSEQS_ERR_ARG;
   if (!fast_domain(false, gap, 0) || !fast_domain(true, gap_open, gap_extend))
     return SSEQS_ERR_UNSUPPORTED;
   SwArgs a{query_idx, query_len, good_idx, g0, n_targets, ascii, delim, 0, out_linear, gap,
@@ -378,6 +385,12 @@ extern "C" int sseqs_sw_set_variant(int affine, int tpt, int wide) {
   std::lock_guard<std::mutex> lk(cache().mu);
   cache().variant[affine][tpt - 1] = wide;
   return SSEQS_OK;
+}
+
+extern "C" int sseqs_sw_get_variant(int affine, int tpt) {
+  if (tpt < 1 || tpt > 64 || affine < 0 || affine > 2) return -1;
+  std::lock_guard<std::mutex> lk(cache().mu);
+  return cache().variant[affine][tpt - 1];
 }
 
 extern "C" int sseqs_sw_variant_words(int affine, int tpt, int wide) {

@@ -207,18 +207,27 @@ def synthetic_db(queries: list[str], n_seqs: int, homolog_frac: float, ident: tu
 
 def pack_symbols_host(sym: np.ndarray) -> np.ndarray:
     """Host xbit packer (layout of sseqs/xbit.cu:36-62), for building files."""
-    sym = np.asarray(sym, dtype=np.uint8)
+    sym = np.asarray(sym, dtype=np.uint8).reshape(-1)
     n = sym.size
     g = (n + 7) // 8
-    pad = np.full(g * 8, 64, np.uint8)
-    pad[:n] = sym
-    s = (pad.reshape(g, 8).astype(np.uint64) - 64) & 31
-    w = np.zeros(g, np.uint64)
-    for k in range(8):
-        w |= s[:, k] << np.uint64(35 - 5 * k)
     out = np.empty((g, 5), np.uint8)
-    for b in range(5):
-        out[:, b] = ((w >> np.uint64(32 - 8 * b)) & np.uint64(255)).astype(np.uint8)
+    step = 1 << 22                       # groups per block
+    for g0 in range(0, g, step):
+        g1 = min(g, g0 + step)
+        blk = np.full((g1 - g0) * 8, 64, np.uint8)
+        part = sym[g0 * 8:min(n, g1 * 8)]
+        blk[:part.size] = part
+        blk -= 64
+        blk &= 31
+        # a group's 8 symbols as one little-endian word: symbol k in byte k;
+        # place symbol k at bit 59 - 5k, so the 40-bit group fills the top
+        # of the word, and byte-swap: its first 5 bytes are the big-endian
+        # packed group
+        x = blk.view("<u8")
+        w = np.zeros_like(x)
+        for k in range(8):
+            w |= ((x >> np.uint64(8 * k)) & np.uint64(31)) << np.uint64(59 - 5 * k)
+        out[g0:g1] = w.byteswap().view(np.uint8).reshape(-1, 8)[:, :5]
     return out.reshape(-1)[: (5 * n + 7) // 8]
 
 

@@ -51,6 +51,8 @@ class BatchHits:
     maxlen: int
     cells_linear: int
     cells_affine: int
+    pos: torch.Tensor | None = None     # position of each hit in the candidate list
+    fft: torch.Tensor | None = None     # prefilter scores of the batch (None: not computed)
 
 
 class SearchStats:
@@ -132,9 +134,10 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
         g = (p3 + 1).to(torch.int32)
     else:
         g = cand2[p3].to(torch.int32)
-    lin_s = lin[p3] if p2 is None else lin[p2.long()[p3]]
+    pos = p3 if p2 is None else p2.long()[p3]
     hits, hlen = _gather_hits(batch, g, k3)
-    return BatchHits(bi, g, aff[p3], lin_s, hits, hlen, batch.maxlen, 0, 0)
+    return BatchHits(bi, g, aff[p3], lin[pos], hits, hlen, batch.maxlen, 0, 0, pos,
+                     None if top_fft == 1 else scores)
 
 
 def _norm(aff: np.ndarray, Lq: int, maxlen: int) -> np.ndarray:
@@ -180,11 +183,49 @@ def rank_hits(query: str, per_batch: list, num_msas: int):
                     c["aff"][keep].tolist(), c["lin"][keep].tolist(), hits))
 
 
+def raw_hits(query: str, per_batch: list):
+    """Every batch's hits in the layout of the reference's ``save_raw`` pickle
+    (sseqs/msa.py:413-422): [query, hit strings, linear scores, prefilter
+    scores, normalised affine scores], batches in order.
+
+    Inside a batch the hits are in the order the reference's top-k calls
+    produce when their ties fall to the lower position: affine score, then
+    linear score (descending), then segment.  The prefilter column repeats
+    the reference's indexing (``scores[good_idx]`` with ``good_idx`` the hit's
+    position in the candidate list, sseqs/msa.py:362-363); with
+    ``top_fft == 1`` no prefilter runs here and the column holds NaN.
+    """
+    matches, lin_all, fft_all, norm_all = [], [], [], []
+    for bh in per_batch:
+        if bh is None or bh.g.numel() == 0:
+            continue
+        g, aff, lin = to_host(bh.g), to_host(bh.affine), to_host(bh.linear)
+        order = np.lexsort((g, -lin.astype(np.int64), -aff.astype(np.int64)))
+        idx = torch.from_numpy(order).to(bh.hits.device)
+        hb, hl = to_host(bh.hits.index_select(0, idx)), to_host(bh.hit_len.index_select(0, idx))
+        w = hb.shape[1]
+        blob = hb.tobytes()
+        for r, n in enumerate(hl.tolist()):
+            matches.append(blob[r * w:r * w + min(max(n, 0), w)].decode("latin-1"))
+        norm = _norm(aff[order], len(query), bh.maxlen)
+        if bh.fft is None:
+            fft = np.full(order.size, np.nan, np.float16)
+        else:
+            fft = to_host(bh.fft.index_select(0, bh.pos.index_select(0, idx)))
+        lin_all.extend(lin[order])
+        fft_all.extend(fft)
+        norm_all.extend(norm)
+    return [query, matches, lin_all, fft_all, norm_all]
+
+
 def search(queries, db: Database | None = None, *, num_msas=4096, top_fft=200, top_sw=10,
            top_sw_affine=2, fft_rank=4, dlength=1e6, stats: SearchStats | None = None,
-           timer=None, bs: int | None = None):
+           timer=None, bs: int | None = None, per_batch_out: list | None = None):
     """Ranked hits of every query: list (per query) of tuples
-    (normalised score, batch, segment, affine, linear, hit string)."""
+    (normalised score, batch, segment, affine, linear, hit string).
+
+    ``per_batch_out``, if given, receives each query's list of per-batch
+    ``BatchHits`` (None for a batch that gave none)."""
     if isinstance(queries, str):
         queries = [queries]
     db = default_database(bs) if db is None else db
@@ -204,6 +245,8 @@ def search(queries, db: Database | None = None, *, num_msas=4096, top_fft=200, t
             if stats is not None:
                 stats.add("t_sw", time.time() - t0)
         out.append(rank_hits(query, per, num_msas))
+        if per_batch_out is not None:
+            per_batch_out.append(per)
     return out
 
 
@@ -235,16 +278,18 @@ def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50
                 os.remove(f)
         stats = SearchStats()
         t0 = time.time()
+        per_batch = [] if save_raw != "" else None
         ranked = search(queries, db, num_msas=num_msas, top_fft=top_fft, top_sw=top_sw,
                         top_sw_affine=top_sw_affine, fft_rank=fft_rank, dlength=dlength,
-                        stats=stats, bs=bs)
+                        stats=stats, bs=bs, per_batch_out=per_batch)
         if sync_time:
             torch.cuda.synchronize()
         stats.add("t_search", time.time() - t0)
-        for query, fname, rows in zip(queries, filenames, ranked):
+        for qi, (query, fname, rows) in enumerate(zip(queries, filenames, ranked)):
             if save_raw != "":
-                pickle.dump([query, [r[5] for r in rows], [r[4] for r in rows], [],
-                             [r[0] for r in rows]], open(save_raw, "wb"))
+                # one file, rewritten per query, as sseqs/msa.py:420-422 does
+                with open(save_raw, "wb") as fh:
+                    pickle.dump(raw_hits(query, per_batch[qi]), fh)
             t1 = time.time()
             if fname is not None:
                 if verbose:

@@ -34,6 +34,14 @@ def set_variant(affine, tpt: int, wide: int) -> None:
     check(lib().sseqs_sw_set_variant(int(affine), int(tpt), int(wide)), "set_variant")
 
 
+def get_variant(affine, tpt: int) -> int:
+    """The layout selected for (kernel, tpt): 0 narrow, 1 wide."""
+    v = lib().sseqs_sw_get_variant(int(affine), int(tpt))
+    if v < 0:
+        raise ValueError(f"no score kernel for mode {affine}, width {tpt}")
+    return v
+
+
 def has_wide(mode: int, tpt: int) -> bool:
     """Whether the kernel of ``mode`` has a wide layout of its own at ``tpt``."""
     words = [lib().sseqs_sw_variant_words(int(mode), int(tpt), w) for w in (0, 1)]

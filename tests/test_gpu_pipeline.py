@@ -12,6 +12,12 @@ from tests import refkernels
 
 pytestmark = pytest.mark.gpu
 
+# Least share of segments whose reference fp16 prefilter score is finite, per
+# case (a B200 measured 1.0 for each case but the last, 0.491 there: the
+# overflow is a property of the reference kernel, not of this build).
+FINITE_SHARE_MIN = {(64, 40): 1.0, (128, 100): 1.0, (256, 180): 1.0, (512, 300): 1.0,
+                    (1024, 180): 1.0, (1024, 600): 0.45}
+
 
 def _db(n_seqs=4000, chunk_bytes=150_000, Lq=180, seed=0, frac=0.02):
     from sseqs_b200 import dbtools
@@ -31,17 +37,34 @@ def _host_batches(syn, bs):
     return out
 
 
-@pytest.mark.parametrize("Lq,maxlen_cap", [(180, None), (600, None), (40, 50)])
-def test_prefilter_matches_float64_oracle(Lq, maxlen_cap):
-    from sseqs_b200 import conv, select, dbtools
-    rng = np.random.default_rng(Lq)
+# (transform length N, query length, longest segment): one case per N the
+# reference instantiates (sseqs/filter.cu:182-312), plus N = 2048 (none there)
+PREFILTER_CASES = [(64, 40, 50), (128, 100, 128), (256, 180, 256), (512, 300, 512),
+                   (1024, 180, 1000), (1024, 600, 1000), (2048, 1500, 1000)]
+
+
+@pytest.mark.parametrize("N,Lq,maxlen", PREFILTER_CASES)
+def test_prefilter_matches_float64_oracle_and_reference(N, Lq, maxlen):
+    """fp32 direct sums vs the float64 restatement (tight), and vs the
+    reference's own fp16 FFT kernel wherever that kernel's score is finite:
+    its spectrum products overflow fp16 for long inputs, so the finite share
+    is printed and asserted, and on the finite scores the values correlate
+    and a 1/10 selection keeps the same segments."""
+    from sseqs_b200 import conv, dbtools
+    rng = np.random.default_rng(N + Lq)
     query = dbtools.random_query(Lq, Lq)
-    lens = rng.integers(5, maxlen_cap or 1000, 700)
+    lens = rng.integers(5, maxlen + 1, 700)
+    lens[0] = maxlen
     segs = [dbtools.random_query(int(n), 100 + i) for i, n in enumerate(lens)]
-    segs[3] = segs[3][:10] + "XXXBZ" + segs[3][10:]
+    for i in range(5, 700, 37):           # planted pieces of the query
+        a = int(rng.integers(0, max(1, Lq - 30)))
+        piece = query[a:a + int(min(len(segs[i]), Lq - a))]
+        segs[i] = piece + segs[i][len(piece):]
+    segs[3] = (segs[3][:10] + "XXXBZ" + segs[3][15:])[:len(segs[3])]
     ascii = np.frombuffer(("@".join(segs) + "@").encode(), np.uint8).copy()
     seg = O.segment(ascii)
     n = conv.transform_length(Lq, int(seg["lengths"].max()))
+    assert n == N
     A, B = O.prefilter_luts(query, 4)
     exp = O.prefilter_scores(query, A, B, ascii, seg["offsets"], seg["lengths"], n, 4)
     luts = conv.prefilter_luts(query, 4)
@@ -50,20 +73,24 @@ def test_prefilter_matches_float64_oracle(Lq, maxlen_cap):
                                 len(seg["lengths"]), n, 4).float().cpu().numpy()
     tol = 2e-3 * np.maximum(1.0, np.abs(exp))
     assert np.all(np.abs(got - exp) <= tol), np.max(np.abs(got - exp) / np.maximum(1, np.abs(exp)))
-    if refkernels.available() and n <= 1024:
-        ref = refkernels.warp_corr(query, A, B, d(ascii), d(seg["offsets"]),
-                                   d(seg["lengths"]), n, 4).float().cpu().numpy()
-        # The reference computes in fp16; its spectrum products overflow for
-        # long inputs, so compare where its scores are finite, loosely, and
-        # compare the candidate sets a top-1/10 selection takes.
-        fin = np.isfinite(ref)
-        print(f"reference prefilter finite on {fin.mean():.3f} of segments (n={n})")
-        if fin.mean() >= 0.9:
-            assert np.corrcoef(ref[fin], exp[fin])[0, 1] > 0.99
-            k = len(exp) // 10
-            a = set(np.argsort(-np.where(fin, ref, -np.inf), kind="stable")[:k])
-            b = set(np.argsort(-got, kind="stable")[:k])
-            assert len(a & b) >= 0.9 * k
+    if N > 1024:
+        return                            # the reference computes nothing at N = 2048
+    if not refkernels.available():
+        pytest.skip("oracle/_ref/libsseqs_ref.so not built")
+    ref = refkernels.warp_corr(query, A, B, d(ascii), d(seg["offsets"]),
+                               d(seg["lengths"]), n, 4).float().cpu().numpy()
+    fin = np.isfinite(ref)
+    k = len(exp) // 10
+    top_ref = set(np.argsort(-np.where(fin, ref, -np.inf), kind="stable")[:k])
+    top_got = set(np.argsort(-got, kind="stable")[:k])
+    overlap = len(top_ref & top_got) / k
+    corr = np.corrcoef(ref[fin], got[fin])[0, 1] if fin.sum() > 2 else float("nan")
+    print(f"N={N} Lq={Lq}: reference finite on {fin.mean():.3f} of segments, "
+          f"corr {corr:.4f} on those, top-1/10 overlap {overlap:.3f}")
+    assert fin.mean() >= FINITE_SHARE_MIN[(N, Lq)]
+    assert corr > 0.99
+    if fin.all():
+        assert overlap >= 0.9
 
 
 def _oracle_search(query, batches, prefilter_fn=None, **kw):

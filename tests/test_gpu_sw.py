@@ -53,25 +53,74 @@ def test_sw_ops_match_oracle(Lq):
     np.testing.assert_array_equal(aff2, O.sw_affine(q, good, ascii, sp, 11, 1, NT))
 
 
-@pytest.mark.parametrize("Lq", [40, 200, 513, 1024])
+# one query length per stripe width 1..32 (the reference's kernels L = 32..1024,
+# sseqs/sw.cu:336-425), with varied remainders
+REF_LENGTHS = [32 * t - (7 * t) % 32 for t in range(1, 33)]
+
+
+class _Variants:
+    """Select lane layouts for a width and put back the ones selected before."""
+
+    def __init__(self, tpt):
+        from sseqs_b200 import tune
+        self.tune, self.tpt = tune, tpt
+        self.before = [tune.get_variant(m, tpt) for m in (0, 1, 2)]
+
+    def set(self, wide):
+        for m in (0, 1, 2):
+            self.tune.set_variant(m, self.tpt, wide)
+
+    def restore(self):
+        for m, w in enumerate(self.before):
+            self.tune.set_variant(m, self.tpt, w)
+
+
+@pytest.mark.parametrize("Lq", REF_LENGTHS)
 def test_sw_ops_match_reference_cuda_kernels(Lq):
+    """Every score kernel of this width -- linear, affine and the fused pass,
+    in each lane layout the width has -- equals the reference's own kernels
+    compiled from source, on both window forms msa() uses."""
     if not refkernels.available():
         pytest.skip("oracle/_ref/libsseqs_ref.so not built")
     S = importlib.import_module("sseqs_b200.sw")
-    query, q, ascii, starts = _case(1000 + Lq, Lq, 700, extra="XB")
-    good = np.arange(1, len(starts), dtype=np.int32)     # g >= 1: defined windows
-    qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
-    for gap in (-1, -4, -11):
-        mine = S.sw_cuda_blosum62(qd, gd, ad, sd, gap_penalty_param=gap)
-        ref = refkernels.sw_linear(qd, gd, ad, sd, gap)
-        torch.testing.assert_close(mine, ref, rtol=0, atol=0)
-    for go, ge in ((11, 1), (5, 2), (0, 0)):
-        mine = S.sw_cuda_affine(qd, gd, ad, sd, go, ge)
-        ref = refkernels.sw_affine(qd, gd, ad, sd, go, ge)
-        torch.testing.assert_close(mine, ref, rtol=0, atol=0)
-    sp = _dev((starts + 1).astype(np.int32))
-    torch.testing.assert_close(S.sw_cuda_affine(qd, gd, ad, sp, 11, 1),
-                               refkernels.sw_affine(qd, gd, ad, sp, 11, 1), rtol=0, atol=0)
+    from sseqs_b200 import tune
+    tpt = tune.tpt_of(Lq)
+    assert tpt == REF_LENGTHS.index(Lq) + 1
+    query, q, ascii, starts = _case(1000 + Lq, Lq, 500 if Lq <= 512 else 300, extra="XB")
+    ascii = np.concatenate([ascii, np.full(48, 64, np.uint8)])
+    delim = np.flatnonzero(ascii == 64).astype(np.int32)
+    nseg = len(starts)
+    good = np.arange(1, nseg, dtype=np.int32)     # g >= 1: defined windows
+    qd, gd, ad, dd = _dev(q), _dev(good), _dev(ascii), _dev(delim)
+    dp = _dev(delim + 1)
+    ref_lin = {gap: refkernels.sw_linear(qd, gd, ad, dd, gap) for gap in (-1, -4, -11)}
+    ref_aff = {p: refkernels.sw_affine(qd, gd, ad, dd, *p) for p in ((11, 1), (5, 2), (0, 0))}
+    ref_shift = refkernels.sw_affine(qd, gd, ad, dp, 11, 1)
+    layouts = [0] + [1 for m in (0, 1, 2) if tune.has_wide(m, tpt)][:1]
+    v = _Variants(tpt)
+    try:
+        for wide in layouts:
+            v.set(wide)
+            for gap, ref in ref_lin.items():
+                torch.testing.assert_close(S.sw_cuda_blosum62(qd, gd, ad, dd, gap), ref,
+                                           rtol=0, atol=0)
+            for (go, ge), ref in ref_aff.items():
+                torch.testing.assert_close(S.sw_cuda_affine(qd, gd, ad, dd, go, ge), ref,
+                                           rtol=0, atol=0)
+            torch.testing.assert_close(S.sw_cuda_affine(qd, gd, ad, dp, 11, 1), ref_shift,
+                                       rtol=0, atol=0)
+            # scan forms: msa()'s linear call (skip 0) and affine call (delim+1 = skip 1)
+            torch.testing.assert_close(
+                S.sw_scan(qd, ad, dd, affine=False, g0=1, n_targets=nseg - 1, skip=0, gap_a=-1),
+                ref_lin[-1], rtol=0, atol=0)
+            torch.testing.assert_close(
+                S.sw_scan(qd, ad, dd, affine=True, g0=1, n_targets=nseg - 1, skip=1, gap_a=11,
+                          gap_b=1), ref_shift, rtol=0, atol=0)
+            lin, aff = S.sw_scan_both(qd, ad, dd, g0=1, n_targets=nseg - 1, affine_skip=1)
+            torch.testing.assert_close(lin, ref_lin[-1], rtol=0, atol=0)
+            torch.testing.assert_close(aff, ref_shift, rtol=0, atol=0)
+    finally:
+        v.restore()
 
 
 def test_scan_matches_reference_windows():
@@ -148,10 +197,10 @@ def test_wide_layout_matches_oracle(Lq):
     good = np.arange(len(starts), dtype=np.int32)
     qd, gd, ad, sd = _dev(q), _dev(good), _dev(ascii), _dev(starts)
     tpt = tune.tpt_of(Lq)
+    v = _Variants(tpt)
     try:
         for wide in (0, 1):
-            tune.set_variant(False, tpt, wide)
-            tune.set_variant(True, tpt, wide)
+            v.set(wide)
             np.testing.assert_array_equal(
                 S.sw_cuda_blosum62(qd, gd, ad, sd, gap_penalty_param=-1).cpu().numpy(),
                 O.sw_linear(q, good, ascii, starts, -1, NT))
@@ -159,35 +208,29 @@ def test_wide_layout_matches_oracle(Lq):
                 S.sw_cuda_affine(qd, gd, ad, sd, 11, 1).cpu().numpy(),
                 O.sw_affine(q, good, ascii, starts, 11, 1, NT))
     finally:
-        tune.set_variant(False, tpt, 0)
-        tune.set_variant(True, tpt, 0)
+        v.restore()
 
 
-
-def _set_variant(mode, tpt, wide):
-    from sseqs_b200 import _lib
-    _lib.check(_lib.lib().sseqs_sw_set_variant(mode, tpt, wide), "set_variant")
-
-
-@pytest.mark.parametrize("Lq", [1, 20, 33, 64, 100, 200, 287, 500, 545, 640, 672, 673, 858, 1000, 1300, 1536,
-                                1537, 2048])
+@pytest.mark.parametrize("Lq", [1, 20, 33, 64, 100, 200, 287, 500, 545, 640, 672, 673, 700, 858,
+                                1000, 1300, 1536, 1537, 2048])
 @pytest.mark.parametrize("wide", [0, 1])
 def test_scan_both_equals_two_scans(Lq, wide):
     """The fused pass gives exactly the linear (skip 0) and affine (skip 1 or
     0) scores of the two separate scans and of the oracle; widths above 48
     words run the two kernels in turn."""
     S = importlib.import_module("sseqs_b200.sw")
+    from sseqs_b200 import tune
     tpt = (Lq + 31) // 32
-    if wide and tpt > 16:
-        pytest.skip("the wide layout exists for widths up to 16")
+    if wide and not any(tune.has_wide(m, tpt) for m in (0, 1, 2)):
+        pytest.skip("no kernel has a wide layout at this width")
     n = 500 if Lq <= 300 else 160
     query, q, ascii, starts = _case(Lq + 3, Lq, n, extra="XBZU*")
     ascii = np.concatenate([ascii, np.full(40, 64, np.uint8)])
     delim = np.flatnonzero(ascii == 64).astype(np.int32)
     nseg = len(delim)
     qd, ad, dd = _dev(q), _dev(ascii), _dev(delim)
-    for mode in (0, 1, 2):
-        _set_variant(mode, tpt, wide)
+    v = _Variants(tpt)
+    v.set(wide)
     try:
         lin, aff = S.sw_scan_both(qd, ad, dd, g0=1, n_targets=nseg - 1, affine_skip=1)
         exp_l = S.sw_scan(qd, ad, dd, affine=False, g0=1, n_targets=nseg - 1, skip=0, gap_a=-1)
@@ -211,8 +254,18 @@ def test_scan_both_equals_two_scans(Lq, wide):
         torch.testing.assert_close(aff2, S.sw_scan(qd, ad, dd, affine=True, good_idx=gd, skip=0,
                                                    gap_a=7, gap_b=2), rtol=0, atol=0)
     finally:
-        for mode in (0, 1, 2):
-            _set_variant(mode, tpt, 0)
+        v.restore()
+
+
+def test_scan_both_empty_query_fills_minus_one():
+    """Query length 0: both outputs -1, as the two scans give (sseqs/sw.cu:73)."""
+    S = importlib.import_module("sseqs_b200.sw")
+    raw = np.frombuffer(b"MKTAYIAK@@QRQ@W@", np.uint8).copy()
+    ascii, dd = _dev(raw), _dev(np.flatnonzero(raw == 64).astype(np.int32))
+    q = torch.zeros(0, dtype=torch.uint8, device="cuda")
+    lin, aff = S.sw_scan_both(q, ascii, dd, g0=1, n_targets=3, affine_skip=1)
+    assert (lin == -1).all() and (aff == -1).all()
+    assert (S.sw_scan(q, ascii, dd, affine=False, g0=1, n_targets=3, skip=0, gap_a=-1) == -1).all()
 
 
 def test_scan_both_degenerate_windows():

@@ -55,6 +55,27 @@ def test_backtrack_matches_oracle_random(seed):
     assert got == exp
 
 
+@pytest.mark.parametrize("Lq", [1000, 1500, 2048])
+def test_backtrack_matches_oracle_long_queries(Lq):
+    """Queries up to the longest the search takes (2048) against hit-length
+    targets (the search keeps 500 residues of a hit, sseqs/msa.py:183):
+    planted homologs of query pieces, random targets, and non-standard
+    letters."""
+    from sseqs_b200.sw import backtrack
+    rng = np.random.default_rng(Lq)
+    query = rand_seq(rng, Lq)
+    targets = []
+    for i in range(24):
+        a = int(rng.integers(0, Lq - 400))
+        piece = query[a:a + int(rng.integers(200, 400))]
+        targets.append(homolog_targets(rng, piece, 1, lo=150, hi=500, frac=1.0)[0][:500])
+    targets += [rand_seq(rng, 500), rand_seq(rng, 499, extra="XBZ*"), query[-500:], query[:500]]
+    got = backtrack(query, targets).to_dicts()
+    best, exp = O.sw_affine_backtrack(query, targets)
+    assert got == exp
+    assert max(best) > 300
+
+
 def test_to_a3m_matches_reference_golden(tmp_path):
     from sseqs_b200.to_a3m import to_a3m
     for k, rec in enumerate(_load("to_a3m.json")):

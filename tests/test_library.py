@@ -94,10 +94,27 @@ def test_score_kernel_registry_matches_dispatch_rules(built_lib):
     assert L.sseqs_sw_variant_words(3, 5, 0) == -1 and L.sseqs_sw_variant_words(0, 65, 0) == -1
 
 
+def test_variant_selection_round_trips(built_lib):
+    """The lane layout chosen per (kernel, width) reads back as set; out of
+    range reads -1.  Host state only, no GPU."""
+    from sseqs_b200 import tune
+    before = tune.get_variant(1, 9)
+    try:
+        for w in (1, 0, 1):
+            tune.set_variant(1, 9, w)
+            assert tune.get_variant(1, 9) == w
+    finally:
+        tune.set_variant(1, 9, before)
+    L = built_lib
+    assert L.sseqs_sw_get_variant(3, 1) == -1 and L.sseqs_sw_get_variant(0, 65) == -1
+
+
 def test_scan_both_argument_checks_without_a_gpu(built_lib):
     """sseqs_sw_scan_both rejects bad arguments on the host, before any
-    CUDA call: a window shift other than 0/1, a missing output, a query
-    outside 1..2048, gaps outside the int16 domain; no targets is a no-op."""
+    CUDA call: a window shift other than 0/1, a missing output, a negative
+    query length or one above 2048, gaps outside the int16 domain; no
+    targets is a no-op.  (Query length 0 fills both outputs with -1 on the
+    GPU, as the separate scans do: ``test_gpu_sw``.)"""
     import ctypes
     from sseqs_b200 import _lib
     L = _lib.lib()
@@ -108,7 +125,7 @@ def test_scan_both_argument_checks_without_a_gpu(built_lib):
                                 None) == 1
     assert L.sseqs_sw_scan_both(fake, 10, None, 0, 5, fake, fake, 1, None, fake, -1, 11, 1,
                                 None) == 1
-    assert L.sseqs_sw_scan_both(fake, 0, None, 0, 5, fake, fake, 1, fake, fake, -1, 11, 1,
+    assert L.sseqs_sw_scan_both(fake, -1, None, 0, 5, fake, fake, 1, fake, fake, -1, 11, 1,
                                 None) == 1
     assert L.sseqs_sw_scan_both(fake, 2049, None, 0, 5, fake, fake, 1, fake, fake, -1, 11, 1,
                                 None) == 2
