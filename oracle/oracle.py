@@ -320,9 +320,12 @@ def search_batch(query: str, ascii: np.ndarray, *, top_fft=1, top_sw=1,
     delim = seg["delim_pos"].astype(np.int32)
     lin = sw_linear(q_idx, cand, ascii, delim, gap=-1, nthreads=os.cpu_count())
     k2 = lin.size // top_sw
-    # canonical: survivors in database-index order, so that ties at the
-    # affine cut go to the lower index (torch.topk leaves them unspecified)
-    top2 = np.sort(topk_canonical(lin, k2))
+    # msa.py:324-335 with top-k ties to the lower position: the affine
+    # candidates come in the linear top-k's order (score descending), so an
+    # affine tie at the cut goes to the higher linear score, then the lower
+    # segment (torch.topk leaves tie order unspecified; this is the order
+    # parity is defined on)
+    top2 = topk_canonical(lin, k2)
     starts = seg["starts"].astype(np.int32)
     aff = sw_affine(q_idx, cand[top2], ascii, starts, 11, 1,
                     nthreads=os.cpu_count())

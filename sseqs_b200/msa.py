@@ -129,7 +129,14 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
     # torch.topk raises when top_sw_affine exceeds the list (msa.py:335);
     # here the list is kept whole instead.
     k3 = min(top_sw_affine, k2)
-    p3 = select.topk_indices(aff, k3).long()
+    # The reference scores the affine candidates in the order its linear
+    # top-k returned them (msa.py:324-332), so with top-k ties falling to the
+    # lower position an affine tie goes to the higher linear score, then to
+    # the lower segment: select on the key (affine, linear).  Both scores lie
+    # in [-1, 11 * 2048], so (affine + 1) * 2^15 + linear + 1 fits in int32.
+    lin_c = lin if p2 is None else lin[p2.long()]
+    key = ((aff + 1) << 15) | (lin_c + 1)
+    p3 = select.topk_indices(key, k3).long()
     if cand2 is None:
         g = (p3 + 1).to(torch.int32)
     else:

@@ -22,7 +22,11 @@ replaced underneath it:
   about half a minute per target on this CPU;
 * tensors the reference puts on 'cuda' are made on the CPU (a torch function
   mode), pinned memory is plain memory, and ``torch.cuda`` streams,
-  ``device`` contexts and ``synchronize`` do nothing.
+  ``device`` contexts and ``synchronize`` do nothing;
+* ``torch.topk`` breaks ties by position (equal values: lower index first),
+  one instance of the order torch leaves unspecified, so that the per-batch
+  cuts (sseqs/msa.py:297, 324, 335) are reproducible: parity is defined on
+  this order.
 
 The database file is the case's 1e9-byte chunk; the reference reads it with
 ``CHUNKS=1`` and searches it with the default ``bs`` (5e7, 20 batches).
@@ -95,8 +99,18 @@ def _stand_ins():
     return load, backtrack
 
 
+def _stable_topk(input, k, dim=-1, largest=True, sorted=True):
+    """torch.topk with ties to the lower index (1-D inputs, as msa() has)."""
+    import torch
+    assert input.dim() == 1 and largest
+    order = torch.sort(input, descending=True, stable=True).indices[:k]
+    return torch.return_types.topk((input[order], order))
+
+
 def _cpu_mode():
-    """Torch function mode: 'cuda' tensors on the CPU, no pinning."""
+    """Torch function mode: 'cuda' tensors on the CPU, no pinning, ties of
+    torch.topk to the lower index."""
+    import torch
     from torch.overrides import TorchFunctionMode
 
     class Mode(TorchFunctionMode):
@@ -108,6 +122,8 @@ def _cpu_mode():
             if kwargs.get("pin_memory"):
                 kwargs["pin_memory"] = False
             name = getattr(func, "__name__", "")
+            if func is torch.topk:
+                return _stable_topk(*args, **kwargs)
             if name == "cuda":
                 return args[0]
             if name == "is_pinned":
