@@ -7,7 +7,9 @@ execute under ``TRITON_INTERPRET=1`` with ``device="cpu"``, and its
 change to the reference source is that the module-level JIT build of the
 CUDA extension (sseqs/sw.py:9) is skipped, since nothing here calls it.
 
-Usage:  python tests/golden/make_triton_golden.py [REF_DIR]
+Usage:  python tests/golden/make_triton_golden.py REF_DIR
+        (or SSEQS_REF=REF_DIR python tests/golden/make_triton_golden.py)
+REF_DIR is the reference's sseqs/ source directory.
 Writes: tests/golden/triton_backtrack.json, tests/golden/to_a3m.json
 """
 import functools
@@ -19,7 +21,7 @@ os.environ["TRITON_INTERPRET"] = "1"
 
 import numpy as np  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/sseqs"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SSEQS_REF", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 AA = "ARNDCQEGHILKMFPSTWYV"
 
@@ -85,6 +87,8 @@ def cases(rng):
 
 
 def main():
+    if not os.path.isfile(os.path.join(REF, "sw.py")):
+        sys.exit("give the reference's sseqs/ directory (argument or SSEQS_REF)")
     bt, to_a3m = load_reference()
     rng = np.random.default_rng(20240601)
     records = []
