@@ -123,7 +123,7 @@ def build_database(queries, db_seqs, seed=0):
     from sseqs_b200 import dbtools
     from sseqs_b200.database import Database
     syn = dbtools.synthetic_db(queries, db_seqs, HOMOLOG_FRAC, IDENT, seed=seed, device="cuda")
-    db = Database(syn.chunks, bs=BS)
+    db = Database(syn.chunks, bs=BS, keep_packed=True)
     info = {"db_sequences": syn.n_seqs, "db_residues": syn.n_residues, "db_chunks": len(syn.chunks),
             "db_packed_bytes": len(syn.chunks) * BS}
     del syn
@@ -369,6 +369,90 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
             "index_rows": index.n, "index_bytes": int(index.codes.numel())}
 
 
+def kernels_one_batch_leg(db, queries):
+    """GCUPS of this build's drop-in score operators (``sw_cuda_blosum62``,
+    gap -1, windows of sseqs/msa.py:313-319; ``sw_cuda_affine``, 11/1,
+    windows of :327-332) over segments 1 .. n-2 of the first database batch,
+    per query of at most 1024 residues: the call form and inputs the
+    reference arm times its own kernels on."""
+    import torch
+    sw = importlib.import_module("sseqs_b200.sw")
+    b = db.batches[0]
+    nseg = b.n_segments
+    good = torch.arange(1, nseg - 1, dtype=torch.int32, device="cuda")
+    residues = int(b.lengths[1:nseg - 1].sum(dtype=torch.int64).item())
+    dp1 = (b.delim + 1).contiguous()
+    lin_ms = aff_ms = 0.0
+    cells = 0
+    qs = [q for q in queries if len(q) <= 1024]
+    for q in qs:
+        qe = sw.encode_query(q)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        sw.sw_cuda_blosum62(qe, good, b.ascii, b.delim, gap_penalty_param=-1)
+        ev[1].record()
+        sw.sw_cuda_affine(qe, good, b.ascii, dp1, 11, 1)
+        ev[2].record()
+        torch.cuda.synchronize()
+        lin_ms += ev[0].elapsed_time(ev[1])
+        aff_ms += ev[1].elapsed_time(ev[2])
+        cells += len(q) * residues
+    return {"gcups_linear": round(cells / (lin_ms * 1e-3) / 1e9, 1),
+            "gcups_affine": round(cells / (aff_ms * 1e-3) / 1e9, 1),
+            "segments": nseg - 2, "residues": residues, "queries": len(qs)}
+
+
+def linear_gap4_leg(db, queries, res_cells):
+    """BLOSUM62 with linear gap 4 (the benchmark's "linear (gap 4)"
+    variant) over every segment 1 .. n-2 of every batch: GCUPS."""
+    import torch
+    sw = importlib.import_module("sseqs_b200.sw")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for q in queries:
+        qe = sw.encode_query(q)
+        for b in db.batches:
+            if b.n_segments > 2:
+                sw.sw_scan(qe, b.ascii, b.delim, affine=False, g0=1, n_targets=b.n_segments - 2,
+                           skip=0, gap_a=-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cells = sum(len(q) for q in queries) * res_cells
+    return {"gcups": round(cells / (ms * 1e-3) / 1e9, 1), "queries": len(queries),
+            "gap": -4}
+
+
+def search_defaults_leg(M, db, queries):
+    """The reference's defaults (bs = 5e7, top_fft = 200, top_sw = 10,
+    top_sw_affine = 2, sseqs/msa.py:71-85) over the whole database: packed
+    database bytes searched per second, the reference's own figure
+    (README.md:11-12: GB/s over its chunk loop; the a3m after the loop is
+    not in it).  The database is decoded once more with bs = 5e7 and stays
+    resident."""
+    import torch
+    from sseqs_b200.database import Database
+    db50 = Database(db.packed, bs=50_000_000)
+    packed = sum(c.numel() for c in db.packed)
+    M.search([queries[-1]], db50, num_msas=TOP_K)            # warm-up (LUTs, first launches)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    hits = 0
+    for q in queries:
+        hits += len(M.search([q], db50, num_msas=TOP_K, top_fft=200, top_sw=10,
+                             top_sw_affine=2)[0])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    del db50
+    torch.cuda.empty_cache()
+    return {"GB_per_s": round(packed * len(queries) / (ms * 1e-3) / 1e9, 2),
+            "ms_per_query": round(ms / len(queries), 1), "queries": len(queries),
+            "packed_bytes": packed, "hits": hits,
+            "settings": "bs=5e7, top_fft=200, top_sw=10, top_sw_affine=2, database resident"}
+
+
 def measured_peak(name):
     """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
     int pipes), in int16x2 lane-instructions per second."""
@@ -587,6 +671,10 @@ def bench_b200(args):
         "gpu_launches": int(n_launch),
         "clocks": clk,
     }
+    if world == 1 and args.reference_legs:
+        out["kernels_one_batch"] = kernels_one_batch_leg(db, timed[:4])
+        out["linear_gap4"] = linear_gap4_leg(db, timed[:2], res_cells)
+        out["search_defaults"] = search_defaults_leg(M, db, timed[:4])
     if world == 1 and args.prefilter_steps > 0:
         out["prefiltered"] = prefiltered_leg(M, db, timed[:args.prefilter_steps], exact_rows)
     if world == 1 and args.batched_queries > 0:
@@ -651,7 +739,45 @@ def bench_reference(args):
         "e2e": {"value": round(gcups, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if args.reference_legs:
+        out["reference_gpu"] = reference_gpu_legs(queries, args)
     print(json.dumps(out), flush=True)
+
+
+def reference_gpu_legs(queries, args):
+    """The reference's own CUDA kernels (oracle/_ref, compiled from its
+    sources) on this GPU, beside the CPU value above: its score kernels over
+    the first batch of the benchmark database (the inputs the b200 arm's
+    ``kernels_one_batch`` leg times), and its search loop at its defaults
+    (oracle/ref_search.py: sseqs/msa.py:196-405 restated around its kernels,
+    the database streamed from pinned host memory as the reference does)."""
+    try:
+        import torch
+        from oracle import ref_search, refkernels
+        if not (torch.cuda.is_available() and refkernels.available()):
+            return {"unavailable": "no GPU or oracle/_ref not built"}
+        from sseqs_b200 import dbtools
+        syn = dbtools.synthetic_db(queries, args.db_seqs, HOMOLOG_FRAC, IDENT, seed=0,
+                                   device="cuda")
+        _, timed = step_queries(queries, args.steps, args.warmup)
+        res = {"kernels_one_batch": ref_search.kernels_one_batch(timed[:4], syn.chunks[0])}
+        pinned = ref_search.pinned_copies(syn.chunks)
+        del syn
+        torch.cuda.empty_cache()
+        ref_search.search_chunks(queries[-1], pinned[:1])             # warm-up
+        t0 = time.time()
+        for q in timed[:4]:
+            ref_search.search_chunks(q, pinned)
+        dt = time.time() - t0
+        packed = sum(p.numel() for p in pinned)
+        res["search_defaults"] = {
+            "GB_per_s": round(packed * 4 / dt / 1e9, 2), "ms_per_query": round(dt * 250, 1),
+            "queries": 4, "packed_bytes": packed,
+            "settings": "bs=5e7, top_fft=200, top_sw=10, top_sw_affine=2, chunks streamed "
+                        "from pinned host memory (the reference's loop)"}
+        return res
+    except Exception as e:      # a measurement aid: report, do not fail the arm
+        return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
 
 
 def main():
@@ -663,6 +789,9 @@ def main():
     ap.add_argument("--db-seqs", type=int, default=DB_SEQS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-legs", dest="reference_legs", action="store_false",
+                    help="skip the legs that time the reference's kernels (reference arm) and "
+                         "this build on the same inputs (b200 arm)")
     ap.add_argument("--prefilter-steps", type=int, default=4,
                     help="queries of the prefiltered (FFT) leg; 0 skips it")
     ap.add_argument("--batched-queries", type=int, default=16,

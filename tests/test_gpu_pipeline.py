@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from tests import refkernels
+from oracle import refkernels
 
 pytestmark = pytest.mark.gpu
 

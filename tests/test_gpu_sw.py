@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from tests import refkernels
+from oracle import refkernels
 from tests.helpers import homolog_targets, rand_seq
 
 pytestmark = pytest.mark.gpu

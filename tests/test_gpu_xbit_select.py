@@ -4,7 +4,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from tests import refkernels
+from oracle import refkernels
 
 pytestmark = pytest.mark.gpu
 
