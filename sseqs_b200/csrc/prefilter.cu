@@ -34,6 +34,26 @@
 // the maximum at once unless its partner c[s+N] exists, in which case it is
 // parked in a per-warp shared array until the segment's last row, when the
 // remaining diagonals (m >= Lt) are read off every column.
+//
+// Tensor-core form (rank k <= 4, N <= 1024, the reference's defaults).
+// Only even lags enter the score, so with lags m = 32u + 2v (row u, column
+// v < 16) and target positions p = kk + 2v,
+//   c[32u + 2v] = sum_r sum_kk a_r[32u - kk] * b_r[kk + 2v],
+// a matrix product C[u, v] = sum_kk A[u, kk] B[kk, v] with
+//   A[u, kk] = a_r[32u - kk]   (the query factors read backwards: a row is 16
+//                                contiguous fp16 of the reversed query, rows
+//                                32 elements apart -- one shared copy per CTA,
+//                                loaded by ldmatrix at any (u, kk) offset),
+//   B[kk, v] = b_r[kk + 2v]    (the segment's factors: a fragment register is
+//                                one aligned half2 of the target array),
+// and the k ranks summed into the same accumulators.  mma.sync m16n8k16
+// (fp16 in, fp32 accumulate): a warp per segment, 16-row tiles of 512 lags,
+// K blocks of 16 target positions that meet the tile's non-zero band only,
+// two 8-column halves per A fragment.  The even-lag sums go to a per-warp
+// shared array, folded there (y[s] = c[s] + c[s+N]) into the maximum.  Work
+// is about (Lq + Lt) * Lt / 2 multiply-adds per rank against Lq * Lt / 2
+// useful ones; the factors are rounded to fp16 (the direct form rounds the
+// profile), sums stay fp32.
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -194,6 +214,222 @@ __global__ void __launch_bounds__(32 * PfShape<C>::WARPS) prefilter_kernel(PfArg
   }
 }
 
+// ------------------------------------------------------- tensor-core form
+constexpr int kMmaRank = 4;            // ranks of the tensor-core form
+constexpr int kMmaMaxN = 1024;         // longest cyclic length (and query, segment)
+constexpr int kMmaTiles = 4;           // 16-row tiles of 512 lags: 2048 >= Lq + len - 1
+constexpr int kQPad = 496;             // zero factors around the query (tile span - 16)
+constexpr int kQLen = 2048;            // per rank, fp16: >= kMmaMaxN + 2 * kQPad + 8
+constexpr int kTOff = 32;              // target factor of position p at [p + kTOff]
+// per rank, fp16: positions -32 .. 128 * ceil((kMmaMaxN + 48) / 128) - 1, the
+// span the fill writes (zero from len on) and the fragments read (< len + 46)
+constexpr int kTLen = kTOff + 128 * ((kMmaMaxN + 48 + 127) / 128);
+constexpr int kLagLen = 16 * 16 * kMmaTiles;       // even lags per warp (fp32)
+
+template <int W>
+struct PfMmaShape {
+  static constexpr size_t q_bytes = sizeof(__half) * kMmaRank * kQLen;
+  // the even-lag sums reuse the target factors' space once the products are done
+  static constexpr size_t warp_bytes = sizeof(__half) * kMmaRank * kTLen;
+  static_assert(warp_bytes >= sizeof(float) * kLagLen && warp_bytes % 16 == 0, "warp space");
+  static constexpr size_t smem = q_bytes + W * warp_bytes + 256 + 16 * sizeof(__half) * 22;
+  static_assert(kQLen % 64 == 0 && kQLen >= kMmaMaxN + 2 * kQPad + 8, "query array");
+};
+
+// The rows of an A fragment are 64 bytes apart, so 16-byte chunk c of a
+// rank's query array is stored at chunk c ^ ((c >> 3) & 3) of its 128-byte
+// line: the 8 rows an ldmatrix reads then fall in 8 different bank groups.
+__device__ __forceinline__ int q_swz(int i) {
+  const int c = i >> 3;
+  return ((c ^ ((c >> 3) & 3)) << 3) | (i & 7);
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t (&r)[4]) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                          uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, "
+      "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int W>
+__global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
+  using S = PfMmaShape<W>;
+  extern __shared__ float4 smem_pf[];
+  __half* qf = reinterpret_cast<__half*>(smem_pf);                     // [4][kQLen]
+  uint8_t* wbase = reinterpret_cast<uint8_t*>(smem_pf) + S::q_bytes;
+  uint8_t* lut = wbase + W * S::warp_bytes;                           // [256]
+  __half* bx = reinterpret_cast<__half*>(lut + 256);                  // [4][22] (pad 16)
+  const int Lq = a.Lq, N = a.N, K = a.k;
+  // reversed query factors: ar_r[x] = a_r[-x] = A_r[qrev[-x]] for -(Lq-1) <= x <= 0,
+  // stored at [x + xoff]; xoff is a multiple of 8 so every ldmatrix row is aligned
+  const int xoff = (Lq - 1 + kQPad + 7) & ~7;
+  for (int i = threadIdx.x; i < kMmaRank * kQLen; i += blockDim.x) {
+    const int r = i / kQLen, li = i - r * kQLen, x = li - xoff;
+    float v = 0.f;
+    if (r < K && x <= 0 && x > -Lq) v = a.A[r * 21 + a.qrev[-x]];
+    qf[r * kQLen + q_swz(li)] = __float2half_rn(v);
+  }
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = (uint8_t)pf_pos((uint8_t)i);
+  for (int i = threadIdx.x; i < kMmaRank * 22; i += blockDim.x) {
+    const int r = i / 22, c = i - r * 22;
+    float v = 0.f;
+    if (r < K) v = c < 21 ? a.B[r * 21 + c] : (r + 1 < K ? a.B[(r + 1) * 21] : 0.f);
+    bx[i] = __float2half_rn(v);
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  __half* tf = reinterpret_cast<__half*>(wbase + wib * S::warp_bytes);     // [4][kTLen]
+  float* lagbuf = reinterpret_cast<float*>(tf);                              // [kLagLen]
+  const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
+  const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
+  const int64_t aoff = (int64_t)(au & 3);
+  const uint32_t qf_s = (uint32_t)__cvta_generic_to_shared(qf);
+  // ldmatrix x4: lane supplies row (lane & 7) + 8 * ((lane >> 3) & 1) of
+  // column block 8 * (lane >> 4)
+  const int lrow = (lane & 7) + 8 * ((lane >> 3) & 1), lcol = 8 * (lane >> 4);
+  const int g = lane >> 2, tq = lane & 3;
+  const int64_t nwarps = (int64_t)gridDim.x * W;
+
+  for (int64_t s = (int64_t)blockIdx.x * W + wib; s < a.n; s += nwarps) {
+    const int len = min((int)a.lengths[s], N);
+    // positions -32 .. -1 are zero (the lag sums of the previous segment
+    // shared this space)
+    for (int i = lane; i < kMmaRank * (kTOff / 2); i += 32)
+      reinterpret_cast<__half2*>(tf + (i / (kTOff / 2)) * kTLen)[i % (kTOff / 2)] =
+          __float2half2_rn(0.f);
+    // target factors b_r[p] for p in [0, len + 48), zero from len on: lane l
+    // takes positions 4(l + 32m) .. +3, from the aligned words w and w + 1
+    // that hold them (w from this lane, w + 1 from the next one); all loads of
+    // the segment are issued before any is used, and a word is read only when
+    // it holds a byte of the segment
+    {
+      constexpr int kM = (kMmaMaxN + 48 + 127) / 128;
+      const int64_t ap = a.offsets[s] + aoff;
+      const int64_t w0 = ap >> 2;
+      const int64_t wend = (ap + len + 3) >> 2;          // words holding segment bytes
+      const uint32_t sh = (uint32_t)(ap & 3) * 8u;
+      const int nm = (len + 48 + 127) / 128;
+      uint32_t w[kM + 1];
+#pragma unroll
+      for (int m = 0; m <= kM; ++m) {
+        const int64_t wi = w0 + lane + 32 * m;
+        w[m] = (m <= nm && wi < wend) ? __ldg(abase + wi) : 0u;
+      }
+#pragma unroll
+      for (int m = 0; m < kM; ++m) {
+        if (m < nm) {
+          uint32_t nx = __shfl_down_sync(0xffffffffu, w[m], 1);
+          const uint32_t wrap = __shfl_sync(0xffffffffu, w[m + 1], 0);
+          if (lane == 31) nx = wrap;
+          const uint32_t raw = __funnelshift_r(w[m], nx, sh);
+          const int p0 = 4 * (lane + 32 * m);
+          int c[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) c[i] = p0 + i < len ? lut[(raw >> (8 * i)) & 0xffu] : -1;
+#pragma unroll
+          for (int r = 0; r < kMmaRank; ++r) {
+            __half h[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) h[i] = c[i] >= 0 ? bx[r * 22 + c[i]] : __float2half_rn(0.f);
+            __half2* dst = reinterpret_cast<__half2*>(tf + r * kTLen + kTOff + p0);
+            dst[0] = __halves2half2(h[0], h[1]);
+            dst[1] = __halves2half2(h[2], h[3]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // lags 0 .. Lq + len - 2 in rows u = lag / 32, tiles of 16 rows
+    const int rows = (Lq + len - 1 + 31) / 32;
+    const int ntiles = (rows + 15) / 16;
+    // two accumulator sets (even and odd ranks) halve the chains of
+    // dependent MMAs
+    float acc[kMmaTiles][2][2][4];
+#pragma unroll
+    for (int ti = 0; ti < kMmaTiles; ++ti)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[ti][0][h][e] = acc[ti][1][h][e] = 0.f;
+    if (len > 0 && Lq > 0) {
+      // kk ranges over [-30, len); tile ti needs kk in (512 ti - Lq, 512 ti + 480]
+      for (int kb = -32; kb < len; kb += 16) {
+        uint32_t bf[kMmaRank][2][2];
+#pragma unroll
+        for (int r = 0; r < kMmaRank; ++r) {
+          const uint32_t* tr = reinterpret_cast<const uint32_t*>(tf + r * kTLen + kTOff + kb);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int v = g + 8 * h;                 // column: lag 32u + 2v
+            bf[r][h][0] = tr[tq + v];               // b[kb + 2tq + 2v .. +1]
+            bf[r][h][1] = tr[tq + v + 4];           // b[kb + 8 + 2tq + 2v .. +1]
+          }
+        }
+#pragma unroll
+        for (int ti = 0; ti < kMmaTiles; ++ti) {
+          if (ti < ntiles && kb + 15 > 512 * ti - Lq && kb <= 512 * ti + 480) {
+#pragma unroll
+            // row u = 16 ti + lrow, columns kb + lcol .. +7: ar[kb + lcol - 32u ...]
+            const uint32_t qa = qf_s + 2u * (uint32_t)q_swz(kb + lcol - 32 * (16 * ti + lrow) + xoff);
+            uint32_t af[kMmaRank][4];
+#pragma unroll
+            for (int r = 0; r < kMmaRank; ++r)
+              if (r < K) ldsm_x4(qa + (uint32_t)(2 * r * kQLen), af[r]);
+#pragma unroll
+            for (int r = 0; r < kMmaRank; ++r) {
+              if (r < K) {
+                mma_16816(acc[ti][r & 1][0], af[r], bf[r][0][0], bf[r][0][1]);
+                mma_16816(acc[ti][r & 1][1], af[r], bf[r][1][0], bf[r][1][1]);
+              }
+            }
+          }
+        }
+      }
+    }
+    // even lag 32u + 2v -> lagbuf[16u + v] (over the target factors: every
+    // lane's reads of them are done)
+    __syncwarp();
+#pragma unroll
+    for (int ti = 0; ti < kMmaTiles; ++ti) {
+      if (ti < ntiles) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int u = 16 * ti + g + 8 * (e >> 1);
+            const int v = 2 * tq + (e & 1) + 8 * h;
+            lagbuf[16 * u + v] = acc[ti][0][h][e] + acc[ti][1][h][e];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // y[s] = c[s] + c[s + N] over even s < N; lags past the computed tiles
+    // are 0, and so are lags no diagonal reaches
+    const int lim = 256 * ntiles;
+    float best = -INFINITY;
+    for (int e1 = lane; e1 < N / 2; e1 += 32) {
+      const int e2 = e1 + N / 2;
+      const float y = (e1 < lim ? lagbuf[e1] : 0.f) + (e2 < lim ? lagbuf[e2] : 0.f);
+      best = fmaxf(best, y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) a.out[s] = __float2half_rn(0.5f * best);
+    __syncwarp();
+  }
+}
+
+constexpr int kMmaWarps = 16;
+
 // ------------------------------------------------------------ dispatch
 using PfFn = void (*)(PfArgs);
 struct PfInfo {
@@ -207,7 +443,25 @@ std::array<PfInfo, sizeof...(I)> pf_table(std::integer_sequence<int, I...>) {
   return {{PfInfo{prefilter_kernel<I + 1>, PfShape<I + 1>::smem, 32 * PfShape<I + 1>::WARPS}...}};
 }
 
+int launch_pf_mma(const PfArgs& a, cudaStream_t stream) {
+  using S = PfMmaShape<kMmaWarps>;
+  const void* fn = (const void*)prefilter_mma_kernel<kMmaWarps>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) !=
+      cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 32 * kMmaWarps, S::smem) !=
+          cudaSuccess || nb < 1)
+    return SSEQS_ERR_CUDA;
+  const int64_t need = (a.n + kMmaWarps - 1) / kMmaWarps;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * nb));
+  { prefilter_mma_kernel<kMmaWarps><<<grid, 32 * kMmaWarps, S::smem, stream>>>(a); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
 int launch_pf(const PfArgs& a, cudaStream_t stream) {
+  if (a.k <= kMmaRank && a.N <= kMmaMaxN && a.Lq >= 1 && a.Lq <= kMmaMaxN)
+    return launch_pf_mma(a, stream);
   static const auto table = pf_table(std::make_integer_sequence<int, 64>{});
   const int C = std::max(1, (a.Lq + 31) / 32);
   const PfInfo& info = table[C - 1];

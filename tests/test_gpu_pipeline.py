@@ -93,6 +93,28 @@ def test_prefilter_matches_float64_oracle_and_reference(N, Lq, maxlen):
         assert overlap >= 0.9
 
 
+@pytest.mark.parametrize("k", [1, 3, 6])
+def test_prefilter_other_ranks_match_float64_oracle(k):
+    """Ranks 1-4 take the tensor-core form, higher ranks the direct form; both
+    give the float64 restatement's scores (rank 1 clamps BLOSUM62 at 0,
+    sseqs/msa.py:125)."""
+    from sseqs_b200 import conv, dbtools
+    rng = np.random.default_rng(k)
+    query = dbtools.random_query(300, k)
+    segs = [dbtools.random_query(int(n), 300 + i) for i, n in enumerate(rng.integers(1, 500, 400))]
+    ascii = np.frombuffer(("@".join(segs) + "@").encode(), np.uint8).copy()
+    seg = O.segment(ascii)
+    n = conv.transform_length(len(query), int(seg["lengths"].max()))
+    A, B = O.prefilter_luts(query, k)
+    exp = O.prefilter_scores(query, A, B, ascii, seg["offsets"], seg["lengths"], n, k)
+    luts = conv.prefilter_luts(query, k)
+    d = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    got = conv.prefilter_scores(luts, d(ascii), d(seg["offsets"]), d(seg["lengths"].astype(np.int32)),
+                                len(seg["lengths"]), n, k).float().cpu().numpy()
+    tol = 2e-3 * np.maximum(1.0, np.abs(exp))
+    assert np.all(np.abs(got - exp) <= tol)
+
+
 def _oracle_search(query, batches, prefilter_fn=None, **kw):
     """Oracle restatement over the non-empty batches (numbered in order)."""
     rows = []
