@@ -35,7 +35,7 @@
 // parked in a per-warp shared array until the segment's last row, when the
 // remaining diagonals (m >= Lt) are read off every column.
 //
-// Tensor-core form (rank k <= 4, N <= 1024, the reference's defaults).
+// Tensor-core form (rank k <= 4, N <= 2048; the reference's default rank is 4).
 // Only even lags enter the score, so with lags m = 32u + 2v (row u, column
 // v < 16) and target positions p = kk + 2v,
 //   c[32u + 2v] = sum_r sum_kk a_r[32u - kk] * b_r[kk + 2v],
@@ -86,6 +86,7 @@ struct PfArgs {
   int k;
   int N;                    // cyclic length
   __half* out;              // [n]
+  int len_lo, len_hi;       // tensor-core form: segments with len_lo < min(len, N) <= len_hi
 };
 
 template <int C>
@@ -216,24 +217,26 @@ __global__ void __launch_bounds__(32 * PfShape<C>::WARPS) prefilter_kernel(PfArg
 
 // ------------------------------------------------------- tensor-core form
 constexpr int kMmaRank = 4;            // ranks of the tensor-core form
-constexpr int kMmaMaxN = 1024;         // longest cyclic length (and query, segment)
-constexpr int kMmaTiles = 4;           // 16-row tiles of 512 lags: 2048 >= Lq + len - 1
+constexpr int kMmaPass = 4;            // 16-row tiles of 512 lags accumulated per pass
 constexpr int kQPad = 496;             // zero factors around the query (tile span - 16)
-constexpr int kQLen = 2048;            // per rank, fp16: >= kMmaMaxN + 2 * kQPad + 8
 constexpr int kTOff = 32;              // target factor of position p at [p + kTOff]
-// per rank, fp16: positions -32 .. 128 * ceil((kMmaMaxN + 48) / 128) - 1, the
-// span the fill writes (zero from len on) and the fragments read (< len + 46)
-constexpr int kTLen = kTOff + 128 * ((kMmaMaxN + 48 + 127) / 128);
-constexpr int kLagLen = 16 * 16 * kMmaTiles;       // even lags per warp (fp32)
 
-template <int W>
+// Sizes for a longest cyclic length (and query, segment) MAXN.
+template <int MAXN, int W>
 struct PfMmaShape {
-  static constexpr size_t q_bytes = sizeof(__half) * kMmaRank * kQLen;
+  // reversed query factors per rank (fp16), whole 128-byte lines
+  static constexpr int QLEN = (MAXN + 2 * kQPad + 8 + 63) / 64 * 64;
+  // target factors per rank (fp16): positions -32 .. 128 * ceil((MAXN + 48) / 128) - 1,
+  // the span the fill writes (zero from len on) and the fragments read (< len + 46)
+  static constexpr int TLEN = kTOff + 128 * ((MAXN + 48 + 127) / 128);
+  // 16-row tiles of 512 lags covering Lq + len - 1 <= 2 MAXN - 1 lags
+  static constexpr int TILES = (2 * MAXN - 1 + 511) / 512;
+  static constexpr int LAGS = 256 * TILES;           // even lags per warp (fp32)
+  static constexpr size_t q_bytes = sizeof(__half) * kMmaRank * QLEN;
   // the even-lag sums reuse the target factors' space once the products are done
-  static constexpr size_t warp_bytes = sizeof(__half) * kMmaRank * kTLen;
-  static_assert(warp_bytes >= sizeof(float) * kLagLen && warp_bytes % 16 == 0, "warp space");
+  static constexpr size_t warp_bytes = sizeof(__half) * kMmaRank * TLEN;
+  static_assert(warp_bytes >= sizeof(float) * LAGS && warp_bytes % 16 == 0, "warp space");
   static constexpr size_t smem = q_bytes + W * warp_bytes + 256 + 16 * sizeof(__half) * 22;
-  static_assert(kQLen % 64 == 0 && kQLen >= kMmaMaxN + 2 * kQPad + 8, "query array");
 };
 
 // The rows of an A fragment are 64 bytes apart, so 16-byte chunk c of a
@@ -258,9 +261,10 @@ __device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4],
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-template <int W>
+template <int MAXN, int W>
 __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
-  using S = PfMmaShape<W>;
+  using S = PfMmaShape<MAXN, W>;
+  constexpr int kQLen = S::QLEN, kTLen = S::TLEN;
   extern __shared__ float4 smem_pf[];
   __half* qf = reinterpret_cast<__half*>(smem_pf);                     // [4][kQLen]
   uint8_t* wbase = reinterpret_cast<uint8_t*>(smem_pf) + S::q_bytes;
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   __half* tf = reinterpret_cast<__half*>(wbase + wib * S::warp_bytes);     // [4][kTLen]
-  float* lagbuf = reinterpret_cast<float*>(tf);                              // [kLagLen]
+  float* lagbuf = reinterpret_cast<float*>(tf);                              // [S::LAGS]
   const uintptr_t au = reinterpret_cast<uintptr_t>(a.ascii);
   const uint32_t* abase = reinterpret_cast<const uint32_t*>(au & ~(uintptr_t)3);
   const int64_t aoff = (int64_t)(au & 3);
@@ -300,6 +304,7 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
 
   for (int64_t s = (int64_t)blockIdx.x * W + wib; s < a.n; s += nwarps) {
     const int len = min((int)a.lengths[s], N);
+    if (len <= a.len_lo || len > a.len_hi) continue;     // another launch scores it
     // positions -32 .. -1 are zero (the lag sums of the previous segment
     // shared this space)
     for (int i = lane; i < kMmaRank * (kTOff / 2); i += 32)
@@ -311,7 +316,7 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
     // the segment are issued before any is used, and a word is read only when
     // it holds a byte of the segment
     {
-      constexpr int kM = (kMmaMaxN + 48 + 127) / 128;
+      constexpr int kM = (MAXN + 48 + 127) / 128;
       const int64_t ap = a.offsets[s] + aoff;
       const int64_t w0 = ap >> 2;
       const int64_t wend = (ap + len + 3) >> 2;          // words holding segment bytes
@@ -347,58 +352,76 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
       }
     }
     __syncwarp();
-    // lags 0 .. Lq + len - 2 in rows u = lag / 32, tiles of 16 rows
+    // lags 0 .. Lq + len - 2 in rows u = lag / 32, tiles of 16 rows, kMmaPass
+    // tiles per pass; each pass's sums stay in registers until the last pass
+    // is done, then go to lagbuf[16u + v] (even lag 32u + 2v), over the
+    // target factors
     const int rows = (Lq + len - 1 + 31) / 32;
     const int ntiles = (rows + 15) / 16;
-    // two accumulator sets (even and odd ranks) halve the chains of
-    // dependent MMAs
-    float acc[kMmaTiles][2][2][4];
+    float sums[S::TILES][2][4];
 #pragma unroll
-    for (int ti = 0; ti < kMmaTiles; ++ti)
+    for (int P = 0; P < S::TILES / kMmaPass; ++P) {
+      const int t0 = P * kMmaPass;
+      if (t0 < ntiles) {
+        // two accumulator sets (even and odd ranks) halve the chains of
+        // dependent MMAs
+        float acc[kMmaPass][2][2][4];
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+        for (int tj = 0; tj < kMmaPass; ++tj)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[ti][0][h][e] = acc[ti][1][h][e] = 0.f;
-    if (len > 0 && Lq > 0) {
-      // kk ranges over [-30, len); tile ti needs kk in (512 ti - Lq, 512 ti + 480]
-      for (int kb = -32; kb < len; kb += 16) {
-        uint32_t bf[kMmaRank][2][2];
+          for (int h = 0; h < 2; ++h)
 #pragma unroll
-        for (int r = 0; r < kMmaRank; ++r) {
-          const uint32_t* tr = reinterpret_cast<const uint32_t*>(tf + r * kTLen + kTOff + kb);
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int v = g + 8 * h;                 // column: lag 32u + 2v
-            bf[r][h][0] = tr[tq + v];               // b[kb + 2tq + 2v .. +1]
-            bf[r][h][1] = tr[tq + v + 4];           // b[kb + 8 + 2tq + 2v .. +1]
-          }
-        }
-#pragma unroll
-        for (int ti = 0; ti < kMmaTiles; ++ti) {
-          if (ti < ntiles && kb + 15 > 512 * ti - Lq && kb <= 512 * ti + 480) {
-#pragma unroll
-            // row u = 16 ti + lrow, columns kb + lcol .. +7: ar[kb + lcol - 32u ...]
-            const uint32_t qa = qf_s + 2u * (uint32_t)q_swz(kb + lcol - 32 * (16 * ti + lrow) + xoff);
-            uint32_t af[kMmaRank][4];
-#pragma unroll
-            for (int r = 0; r < kMmaRank; ++r)
-              if (r < K) ldsm_x4(qa + (uint32_t)(2 * r * kQLen), af[r]);
+            for (int e = 0; e < 4; ++e) acc[tj][0][h][e] = acc[tj][1][h][e] = 0.f;
+        if (len > 0) {
+          // kk ranges over [-30, len); tile ti needs kk in (512 ti - Lq, 512 ti + 480]
+          const int kb_lo = max(-32, ((512 * t0 - Lq - 14) >> 4) << 4);
+          const int kb_hi = min(len - 1, 512 * (t0 + kMmaPass - 1) + 480);
+          for (int kb = kb_lo; kb <= kb_hi; kb += 16) {
+            uint32_t bf[kMmaRank][2][2];
 #pragma unroll
             for (int r = 0; r < kMmaRank; ++r) {
-              if (r < K) {
-                mma_16816(acc[ti][r & 1][0], af[r], bf[r][0][0], bf[r][0][1]);
-                mma_16816(acc[ti][r & 1][1], af[r], bf[r][1][0], bf[r][1][1]);
+              const uint32_t* tr =
+                  reinterpret_cast<const uint32_t*>(tf + r * kTLen + kTOff + kb);
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int v = g + 8 * h;             // column: lag 32u + 2v
+                bf[r][h][0] = tr[tq + v];           // b[kb + 2tq + 2v .. +1]
+                bf[r][h][1] = tr[tq + v + 4];       // b[kb + 8 + 2tq + 2v .. +1]
+              }
+            }
+#pragma unroll
+            for (int tj = 0; tj < kMmaPass; ++tj) {
+              const int ti = t0 + tj;
+              if (ti < ntiles && kb + 15 > 512 * ti - Lq && kb <= 512 * ti + 480) {
+                // row u = 16 ti + lrow, columns kb + lcol .. +7: ar[kb + lcol - 32u ...]
+                const uint32_t qa =
+                    qf_s + 2u * (uint32_t)q_swz(kb + lcol - 32 * (16 * ti + lrow) + xoff);
+                uint32_t af[kMmaRank][4];
+#pragma unroll
+                for (int r = 0; r < kMmaRank; ++r)
+                  if (r < K) ldsm_x4(qa + (uint32_t)(2 * r * kQLen), af[r]);
+#pragma unroll
+                for (int r = 0; r < kMmaRank; ++r) {
+                  if (r < K) {
+                    mma_16816(acc[tj][r & 1][0], af[r], bf[r][0][0], bf[r][0][1]);
+                    mma_16816(acc[tj][r & 1][1], af[r], bf[r][1][0], bf[r][1][1]);
+                  }
+                }
               }
             }
           }
         }
+#pragma unroll
+        for (int tj = 0; tj < kMmaPass; ++tj)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) sums[t0 + tj][h][e] = acc[tj][0][h][e] + acc[tj][1][h][e];
       }
     }
-    // even lag 32u + 2v -> lagbuf[16u + v] (over the target factors: every
-    // lane's reads of them are done)
-    __syncwarp();
+    __syncwarp();                                // every lane's factor reads are done
 #pragma unroll
-    for (int ti = 0; ti < kMmaTiles; ++ti) {
+    for (int ti = 0; ti < S::TILES; ++ti) {
       if (ti < ntiles) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -406,7 +429,7 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
           for (int e = 0; e < 4; ++e) {
             const int u = 16 * ti + g + 8 * (e >> 1);
             const int v = 2 * tq + (e & 1) + 8 * h;
-            lagbuf[16 * u + v] = acc[ti][0][h][e] + acc[ti][1][h][e];
+            lagbuf[16 * u + v] = sums[ti][h][e];
           }
         }
       }
@@ -428,7 +451,23 @@ __global__ void __launch_bounds__(32 * W) prefilter_mma_kernel(PfArgs a) {
   }
 }
 
-constexpr int kMmaWarps = 16;
+template <int MAXN, int W>
+int launch_pf_mma(const PfArgs& a, cudaStream_t stream) {
+  using S = PfMmaShape<MAXN, W>;
+  static_assert(S::TILES % kMmaPass == 0, "whole passes");
+  const void* fn = (const void*)prefilter_mma_kernel<MAXN, W>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) !=
+      cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 32 * W, S::smem) != cudaSuccess ||
+      nb < 1)
+    return SSEQS_ERR_CUDA;
+  const int64_t need = (a.n + W - 1) / W;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * nb));
+  { prefilter_mma_kernel<MAXN, W><<<grid, 32 * W, S::smem, stream>>>(a); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
 
 // ------------------------------------------------------------ dispatch
 using PfFn = void (*)(PfArgs);
@@ -443,25 +482,26 @@ std::array<PfInfo, sizeof...(I)> pf_table(std::integer_sequence<int, I...>) {
   return {{PfInfo{prefilter_kernel<I + 1>, PfShape<I + 1>::smem, 32 * PfShape<I + 1>::WARPS}...}};
 }
 
-int launch_pf_mma(const PfArgs& a, cudaStream_t stream) {
-  using S = PfMmaShape<kMmaWarps>;
-  const void* fn = (const void*)prefilter_mma_kernel<kMmaWarps>;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) !=
-      cudaSuccess)
-    return SSEQS_ERR_CUDA;
-  int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, 32 * kMmaWarps, S::smem) !=
-          cudaSuccess || nb < 1)
-    return SSEQS_ERR_CUDA;
-  const int64_t need = (a.n + kMmaWarps - 1) / kMmaWarps;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)device_sm_count() * nb));
-  { prefilter_mma_kernel<kMmaWarps><<<grid, 32 * kMmaWarps, S::smem, stream>>>(a); count_launches(1); }
-  return status_of(cudaGetLastError());
-}
-
 int launch_pf(const PfArgs& a, cudaStream_t stream) {
-  if (a.k <= kMmaRank && a.N <= kMmaMaxN && a.Lq >= 1 && a.Lq <= kMmaMaxN)
-    return launch_pf_mma(a, stream);
+  // tensor-core form for ranks up to 4: segments and queries up to 1024
+  // residues with 16 warps per CTA; longer ones (cyclic length 2048) with the
+  // bigger buffers of the 2048 form, 8 warps per CTA
+  if (a.k <= kMmaRank && a.Lq >= 1 && a.N <= 2048) {
+    if (a.Lq <= 1024) {
+      PfArgs b = a;
+      b.len_lo = -1;
+      b.len_hi = 1024;
+      const int st = launch_pf_mma<1024, 16>(b, stream);
+      if (st != SSEQS_OK || a.N <= 1024) return st;
+      b.len_lo = 1024;
+      b.len_hi = a.N;
+      return launch_pf_mma<2048, 8>(b, stream);
+    }
+    PfArgs b = a;
+    b.len_lo = -1;
+    b.len_hi = a.N;
+    return launch_pf_mma<2048, 8>(b, stream);
+  }
   static const auto table = pf_table(std::make_integer_sequence<int, 64>{});
   const int C = std::max(1, (a.Lq + 31) / 32);
   const PfInfo& info = table[C - 1];
@@ -502,6 +542,6 @@ extern "C" int sseqs_prefilter(const uint8_t* ascii, const int64_t* offsets, con
   if (!workspace || ws_bytes < sseqs_prefilter_workspace_bytes(n, k)) return SSEQS_ERR_WORKSPACE;
   if (n_segments == 0) return SSEQS_OK;
   PfArgs a{ascii, offsets, lengths, n_segments, lut_a, lut_b, query_pos_reversed, query_len, k, n,
-           reinterpret_cast<__half*>(out_scores)};
+           reinterpret_cast<__half*>(out_scores), -1, n};
   return launch_pf(a, stream);
 }

@@ -39,8 +39,10 @@ def _host_batches(syn, bs):
 
 # (transform length N, query length, longest segment): one case per N the
 # reference instantiates (sseqs/filter.cu:182-312), plus N = 2048 (none there)
+# with the query or a segment longer than 1024
 PREFILTER_CASES = [(64, 40, 50), (128, 100, 128), (256, 180, 256), (512, 300, 512),
-                   (1024, 180, 1000), (1024, 600, 1000), (2048, 1500, 1000)]
+                   (1024, 180, 1000), (1024, 600, 1000), (2048, 1500, 1000),
+                   (2048, 300, 1800), (2048, 2000, 2048)]
 
 
 @pytest.mark.parametrize("N,Lq,maxlen", PREFILTER_CASES)
