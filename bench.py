@@ -214,6 +214,7 @@ def batched_leg(db, n_queries, seed=3):
             ln = b.lengths[1:b.n_segments - 1].to(torch.int64)
             rows_aff += int((ln - 1).clamp_(min=0).sum().item())
     cells = int(sum(int(L) for L in lengths)) * rows_aff
+    from sseqs_b200 import tune
     searcher = batched.BatchedSearcher(db, top_k=TOP_K)
     searcher.search(queries)                         # autotune + graph capture
     torch.cuda.synchronize()
@@ -223,6 +224,20 @@ def batched_leg(db, n_queries, seed=3):
     e1.record()
     torch.cuda.synchronize()
     ms_b = e0.elapsed_time(e1)
+    # the same batched launches with one query per launch row at every width
+    pairing = {t: tune.get_query_pairing(t) for t in range(1, 65)}
+    tune.set_query_pairing(0, False)
+    unpaired = batched.BatchedSearcher(db, top_k=TOP_K, autotune=False)
+    unpaired.search(queries)
+    torch.cuda.synchronize()
+    e0.record()
+    got_u = unpaired.search(queries)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_u = e0.elapsed_time(e1)
+    for t, on in pairing.items():
+        tune.set_query_pairing(t, on)
+    del unpaired
 
     def one(q):
         enc = sw.encode_query(q)
@@ -244,7 +259,8 @@ def batched_leg(db, n_queries, seed=3):
     e1.record()
     torch.cuda.synchronize()
     ms_q = e0.elapsed_time(e1)
-    same = True
+    same = all(np.array_equal(a.scores, b.scores) and np.array_equal(a.batch, b.batch)
+               and np.array_equal(a.segment, b.segment) for a, b in zip(got, got_u))
     for h, rows in zip(got, ref):
         sc = np.concatenate([r[0].cpu().numpy() for r in rows])
         bt = np.concatenate([np.full(r[0].numel(), r[1], np.int32) for r in rows])
@@ -258,8 +274,10 @@ def batched_leg(db, n_queries, seed=3):
             "buckets": len(batched.buckets([int(L) for L in lengths])),
             "graphs": len(searcher.plans),
             "gcups_batched": round(cells / (ms_b * 1e-3) / 1e9, 1),
+            "gcups_batched_one_query_per_row": round(cells / (ms_u * 1e-3) / 1e9, 1),
             "gcups_one_query_at_a_time": round(cells / (ms_q * 1e-3) / 1e9, 1),
             "ms_batched": round(ms_b, 1), "ms_one_query_at_a_time": round(ms_q, 1),
+            "paired_widths": sorted(t for t, on in pairing.items() if on),
             "cells": cells, "identical_hits": bool(same)}
 
 

@@ -133,7 +133,12 @@ int sseqs_sw_scan_both(const uint8_t* query_idx, int query_len, const int32_t* g
  * gap <= 0; affine 0 <= open, extend <= 16384), else SSEQS_ERR_UNSUPPORTED.
  * Every query's scores are identical to its own sseqs_sw_scan call.  The
  * lengths are read on the device, so a captured CUDA graph can be replayed
- * with other queries of the same width. */
+ * with other queries of the same width.
+ * Affine queries that share their targets (good_idx null or idx_stride 0)
+ * are scored two per launch row: query 2y in the low and query 2y + 1 in the
+ * high half of every int16x2 word, one target fetch and profile-row load for
+ * both, at the widths sseqs_sw_set_query_pairing selects; scores are the
+ * same. */
 int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const uint8_t* queries,
                           int64_t query_stride, const int32_t* query_lens,
                           const int32_t* good_idx, int64_t idx_stride, int32_t g0,
@@ -273,9 +278,19 @@ int64_t sseqs_launch_count(void);
 /* The score kernel has two lane layouts for stripe widths tpt =
  * ceil(query_len/32) <= 16: narrow (wide = 0, default) and wide (wide = 1:
  * twice the columns per lane, twice the targets per warp).  Selects the one
- * used for (affine, tpt); both give identical scores.  No reference
+ * used for (affine, tpt) -- affine 0 linear, 1 affine, 2 the fused pass, 3
+ * the query-pair kernel of sseqs_sw_scan_queries; both give identical
+ * scores.  No reference
  * counterpart (the autotuner of the batched path sets it). */
 int sseqs_sw_set_variant(int affine, int tpt, int wide);
+/* Whether sseqs_sw_scan_queries scores affine queries of stripe width tpt
+ * (0: every width) that share their targets two per launch row (on = 1) or
+ * one (0, the default until the autotuner of the batched path has timed
+ * both); scores are the same either way.  The getter returns the setting,
+ * or -1 for a width out of range.  No reference counterpart (the reference
+ * scores one query at a time). */
+int sseqs_sw_set_query_pairing(int tpt, int on);
+int sseqs_sw_get_query_pairing(int tpt);
 /* The layout currently selected for (affine, tpt): 0 or 1; -1 if out of
  * range.  No reference counterpart. */
 int sseqs_sw_get_variant(int affine, int tpt);

@@ -73,6 +73,8 @@ _SIGNATURES = {
     "sseqs_kth_largest_rows": (_I, [_P, _I, _I, _I, _P, _P]),
     "sseqs_sw_variant_words": (_I, [_I, _I, _I]),
     "sseqs_sw_get_variant": (_I, [_I, _I]),
+    "sseqs_sw_set_query_pairing": (_I, [_I, _I]),
+    "sseqs_sw_get_query_pairing": (_I, [_I]),
 }
 
 _lock = threading.Lock()

@@ -181,6 +181,7 @@ class BatchedSearcher:
                 raise ValueError(f"query length {L} outside 1..{MAX_QUERY}")
         if self.autotune and db.batches:
             tune.autotune(lengths, db.batches[0])
+            tune.autotune_pairing(lengths, db.batches[0])
         per_query: list = [None] * len(enc)
         for tpt, members in buckets(lengths).items():
             for s in range(0, len(members), self.group):

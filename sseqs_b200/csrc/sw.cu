@@ -90,8 +90,9 @@ const Tables& tables() {
 
 struct Cache {
   std::mutex mu;
-  int max_blocks[2][3][64][64] = {};  // [variant][mode][TPT-1][device]
-  int variant[3][64] = {};            // chosen variant per [mode][TPT-1]
+  int max_blocks[2][kModes][64][64] = {};  // [variant][mode][TPT-1][device]
+  int variant[kModes][64] = {};            // chosen variant per [mode][TPT-1]
+  bool pairing[64] = {};                   // per [TPT-1]: batched affine launches pair queries
 };
 Cache& cache() {
   static Cache c;
@@ -147,7 +148,7 @@ int launch_stream(SwArgs a, int mode, const QueryTable* qt, cudaStream_t stream)
   const int64_t full = (int64_t)device_sm_count() * blocks_per_sm;
   QueryTable none{};
   const QueryTable& table = qt ? *qt : none;
-  const int ny = qt ? qt->n : 1;
+  const int ny = qt ? (mode == kPair ? (qt->n + 1) / 2 : qt->n) : 1;
   unsigned int* const tickets = a.ticket;
   // The kernel counts targets in 32 bits: launches take at most 2^30 each.
   constexpr int64_t kPiece = int64_t(1) << 30;
@@ -353,9 +354,20 @@ extern "C" int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const u
   if (tpt < 1 || tpt > kMaxQuery / 32) return SSEQS_ERR_UNSUPPORTED;
   const bool aff = affine != 0;
   if (!fast_domain(aff, gap_a, gap_b)) return SSEQS_ERR_UNSUPPORTED;
-  for (int q0 = 0; q0 < n_queries; q0 += kMaxLaunchQueries) {
+  // affine queries that share their targets are scored two per launch row
+  // (the query-pair kernel); per-query target lists keep one query per row
+  bool pair;
+  {
+    std::lock_guard<std::mutex> lk(cache().mu);
+    pair = cache().pairing[tpt - 1];
+  }
+  pair = pair && aff && n_queries >= 2 && (!good_idx || idx_stride == 0);
+  // launches of up to kMaxLaunchQueries queries; with pairing, an odd
+  // query left over at the end runs in a one-query-per-row launch (a pair
+  // row with an empty half would cost as much as a full one)
+  auto launch = [&](int q0, int nq, int mode) {
     QueryTable qt{};
-    qt.n = std::min(kMaxLaunchQueries, n_queries - q0);
+    qt.n = nq;
     qt.lens = query_lens + q0;
     qt.q_stride = (int32_t)query_stride;
     qt.out_stride = out_stride;
@@ -363,10 +375,32 @@ extern "C" int sseqs_sw_scan_queries(int affine, int n_queries, int tpt, const u
     const int32_t* idx0 = good_idx ? good_idx + q0 * qt.idx_stride : nullptr;
     SwArgs a{queries + (size_t)q0 * query_stride, tpt * 32, idx0, g0, n_targets,
              ascii, delim, skip, out + q0 * out_stride, gap_a, gap_b, tickets + q0};
-    const int st = launch_stream(a, aff ? kAff : kLin, &qt, stream);
+    return launch_stream(a, mode, &qt, stream);
+  };
+  const int n_paired = pair ? (n_queries & ~1) : 0;
+  for (int q0 = 0; q0 < n_paired; q0 += kMaxLaunchQueries) {
+    const int st = launch(q0, std::min(kMaxLaunchQueries, n_paired - q0), kPair);
+    if (st != SSEQS_OK) return st;
+  }
+  for (int q0 = n_paired; q0 < n_queries; q0 += kMaxLaunchQueries) {
+    const int st = launch(q0, std::min(kMaxLaunchQueries, n_queries - q0), aff ? kAff : kLin);
     if (st != SSEQS_OK) return st;
   }
   return SSEQS_OK;
+}
+
+extern "C" int sseqs_sw_set_query_pairing(int tpt, int on) {
+  if ((on != 0 && on != 1) || tpt < 0 || tpt > 64) return SSEQS_ERR_ARG;
+  std::lock_guard<std::mutex> lk(cache().mu);
+  for (int t = 1; t <= 64; ++t)
+    if (tpt == 0 || t == tpt) cache().pairing[t - 1] = on != 0;
+  return SSEQS_OK;
+}
+
+extern "C" int sseqs_sw_get_query_pairing(int tpt) {
+  if (tpt < 1 || tpt > 64) return -1;
+  std::lock_guard<std::mutex> lk(cache().mu);
+  return cache().pairing[tpt - 1] ? 1 : 0;
 }
 
 extern "C" int sseqs_dpx_peak(uint32_t* sink, double* lane_ops_per_s, cudaStream_t stream) {
@@ -380,7 +414,7 @@ extern "C" int sseqs_int16x2_peak(uint32_t* sink, double* lane_ops_per_s, cudaSt
 }
 
 extern "C" int sseqs_sw_set_variant(int affine, int tpt, int wide) {
-  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine > 2)
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine >= kModes)
     return SSEQS_ERR_ARG;
   std::lock_guard<std::mutex> lk(cache().mu);
   cache().variant[affine][tpt - 1] = wide;
@@ -388,12 +422,12 @@ extern "C" int sseqs_sw_set_variant(int affine, int tpt, int wide) {
 }
 
 extern "C" int sseqs_sw_get_variant(int affine, int tpt) {
-  if (tpt < 1 || tpt > 64 || affine < 0 || affine > 2) return -1;
+  if (tpt < 1 || tpt > 64 || affine < 0 || affine >= kModes) return -1;
   std::lock_guard<std::mutex> lk(cache().mu);
   return cache().variant[affine][tpt - 1];
 }
 
 extern "C" int sseqs_sw_variant_words(int affine, int tpt, int wide) {
-  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine > 2) return -1;
+  if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine >= kModes) return -1;
   return tables().k[wide][affine][tpt - 1].words;
 }

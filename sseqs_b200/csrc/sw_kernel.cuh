@@ -65,7 +65,7 @@ constexpr int kMaxQuery = 2048;
 // register caps without spilling at widths 9-13 and 18-21 only.
 template <int MODE, int TPT, int W>
 __host__ __device__ constexpr int rows_per_fetch() {
-  return MODE == 1 ? (W * TPT <= 16 ? 16 : 8)
+  return (MODE == 1 || MODE == 3) ? (W * TPT <= 16 ? 16 : 8)
        : MODE == 0 && ((W == 1 && TPT <= 13) || (W == 2 && TPT > 16)) ? 8
        : MODE == 2 && W == 1 && (TPT <= 13 || (TPT >= 18 && TPT <= 21)) ? 8 : 4;
 }
@@ -169,10 +169,12 @@ constexpr int words_for() {
 template <int TPT, int W, int MODE>
 constexpr bool vector_major() { return W == 1 || (MODE == 0 && W == 2 && TPT > 18); }
 
-template <int TPT, int W, bool VM>
+template <int TPT, int W, bool VM, bool PAIR = false>
 struct Layout {
-  static constexpr int G = 32 / (2 * W);    // lanes per target
-  static constexpr int GPW = 2 * W;         // targets per warp
+  // lanes per target: a lane holds 2W stripes (two per word), or W stripes
+  // of two queries in the query-pair mode
+  static constexpr int G = PAIR ? 32 / W : 32 / (2 * W);
+  static constexpr int GPW = 32 / G;        // targets per warp
   static constexpr int NWD = W * TPT;       // profile words per lane and row
   static constexpr int NV = (NWD + 3) / 4;  // 128-bit loads per lane and row
   static constexpr int LWP = VM ? NV * 4 : ((NV % 2) ? NV : NV + 1) * 4;  // words per lane
@@ -199,6 +201,15 @@ constexpr int lin_alu_every() { return TPT >= 9 && (TPT < 17 || TPT > 18) ? 4 : 
 // the bookkeeping, and lets the linear recurrence -- FMA-pipe heavy -- fill
 // the ALU pipe slack the affine one leaves, and vice versa).
 constexpr int kLin = 0, kAff = 1, kBoth = 2;
+// Query-pair mode: the affine recurrence of two queries of the same stripe
+// width against the same targets, the lo half of every word holding stripe m
+// of query A and the hi half stripe m of query B.  The two share the byte
+// fetch, the class of every row, the profile-row load and the bookkeeping;
+// and since both halves of a word belong to the same stripe, the diagonal
+// input of a stripe's first column is simply the previous word (no byte
+// permute across halves).
+constexpr int kPair = 3;
+constexpr int kModes = 4;
 
 // Block shape per instantiation.  The state of a lane is about NWD words
 // (linear: H; affine: D and Iy; both: all three) plus its profile rows, so
@@ -213,10 +224,13 @@ constexpr int kLin = 0, kAff = 1, kBoth = 2;
 template <int TPT, int W, int MODE>
 struct Shape {
   static constexpr int NWD = W * TPT;
-  static constexpr int est_regs = MODE == kAff ? 3 * NWD + 32
+  static constexpr int est_regs = (MODE == kAff || MODE == kPair) ? 3 * NWD + 32
                                 : MODE == kLin ? 2 * NWD + 53 : 5 * NWD + 40;
-  static constexpr bool cap85 =
-      est_regs <= 85 && !(MODE == kAff && rows_per_fetch<MODE, TPT, W>() == 8);
+  // (the query-pair kernel carries query B's row and flags besides: it
+  // spilled under the 85-register cap at 12 and 16 words per lane, so it
+  // takes the cap up to 10)
+  static constexpr bool cap85 = est_regs <= 85 && (MODE != kPair || NWD <= 10) &&
+                                !(MODE == kAff && rows_per_fetch<MODE, TPT, W>() == 8);
   static constexpr int threads = est_regs <= 128 ? 256 : 128;
   static constexpr int min_blocks =
       threads == 256 ? (cap85 ? 3 : 2)
@@ -227,11 +241,43 @@ struct Shape {
 template <int TPT, int W, int MODE>
 __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MODE>::min_blocks)
     sw_stream_kernel(SwArgs a, const QueryTable qt) {
+  constexpr bool PAIR = MODE == kPair;
   constexpr bool VM = vector_major<TPT, W, MODE>();
-  using L = Layout<TPT, W, VM>;
-  constexpr bool DO_LIN = MODE != kAff, DO_AFF = MODE != kLin;
+  using L = Layout<TPT, W, VM, PAIR>;
+  constexpr bool DO_LIN = MODE == kLin || MODE == kBoth, DO_AFF = MODE != kLin;
   constexpr int NTAB = MODE == kBoth ? 2 : 1;
-  if (qt.n > 0) {
+  // query-pair mode: query B's residues, length and output row
+  const uint8_t* qB = nullptr;
+  int LqB = 0;
+  int32_t* outB = nullptr;
+  bool writeA = true, writeB = false;
+  if constexpr (PAIR) {
+    // blockIdx.y picks the pair (queries 2y and 2y + 1 of the table); a
+    // query whose length does not belong to this width is not scored (its
+    // row is filled with INT32_MIN) and its half runs on padding
+    const int y = blockIdx.y, ia = 2 * y, ib = 2 * y + 1;
+    const bool hasB = ib < qt.n;
+    const int lenA = qt.lens[ia], lenB = hasB ? qt.lens[ib] : 0;
+    const bool okA = lenA >= 1 && (lenA + 31) / 32 == TPT && lenA <= qt.q_stride;
+    const bool okB = hasB && lenB >= 1 && (lenB + 31) / 32 == TPT && lenB <= qt.q_stride;
+    a.q += (size_t)ia * qt.q_stride;
+    qB = a.q + qt.q_stride;
+    a.out += (int64_t)ia * qt.out_stride;
+    outB = a.out + qt.out_stride;
+    a.ticket += y;
+    if (!okA || (hasB && !okB)) {
+      for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+           i += (int64_t)gridDim.x * blockDim.x) {
+        if (!okA) a.out[i] = INT32_MIN;
+        if (hasB && !okB) outB[i] = INT32_MIN;
+      }
+    }
+    if (!okA && !okB) return;
+    writeA = okA;
+    writeB = okB;
+    a.Lq = okA ? lenA : 0;
+    LqB = okB ? lenB : 0;
+  } else if (qt.n > 0) {
     const int y = blockIdx.y;
     const int len = qt.lens[y];
     a.q += (size_t)y * qt.q_stride;
@@ -257,8 +303,9 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   // Gap parameters: linear gap (p0); affine open and extend (p0, p1 in the
   // affine kernel; p1, p2 in the fused one).
   const int gap = a.p0;
-  const int open = MODE == kAff ? a.p0 : a.p1;
-  const int ext = MODE == kAff ? a.p1 : a.p2;
+  constexpr bool AFF_ONLY = MODE == kAff || MODE == kPair;   // affine gaps in p0, p1
+  const int open = AFF_ONLY ? a.p0 : a.p1;
+  const int ext = AFF_ONLY ? a.p1 : a.p2;
 
   // Profile words.  Affine: s (real columns), -32768 + open (padding), so
   // that M' - open never leaves int16.  Linear: s - gap (the state carries
@@ -266,14 +313,22 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = ascii_class((uint8_t)i);
   for (int i = threadIdx.x; i < NTAB * kNumCls * L::CLS; i += blockDim.x) {
     const int tb = i / (kNumCls * L::CLS), ii = i - tb * (kNumCls * L::CLS);
-    const bool aff_tab = MODE == kAff || tb == 1;
+    const bool aff_tab = AFF_ONLY || tb == 1;
     const int pad = aff_tab ? kNeg + open : -16384;
     const int c = ii / L::CLS, r = ii - c * L::CLS;
     const int slot = r >> 2;                          // uint4 slot in the class
     const int gl = VM ? slot % G : slot / L::LANE_STEP;
     const int v = (VM ? slot / G : slot % L::LANE_STEP) * 4 + (r & 3);   // word of lane gl
     uint32_t word = pack2(pad, pad);
-    if (v < L::NWD) {
+    if (PAIR && v < L::NWD) {
+      // stripe m = gl * W + w of query A (lo) and query B (hi)
+      const int w = v / TPT, k = v - w * TPT;
+      const int j = (gl * W + w) * TPT + k;
+      int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(qB, LqB, c, j);
+      s0 = (s0 == kNeg) ? pad : s0;
+      s1 = (s1 == kNeg) ? pad : s1;
+      word = pack2(s0, s1);
+    } else if (v < L::NWD) {
       const int w = v / TPT, k = v - w * TPT;
       const int j = (gl * 2 * W + 2 * w) * TPT + k;
       int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + TPT);
@@ -387,8 +442,10 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
     if (gl == 0) from_left = 0u;                    // column -1 of stripe 0
     uint32_t din[WA];                               // diagonals, from the previous row
 #pragma unroll
-    for (int w = 0; w < WA; ++w)
-      din[w] = __byte_perm(w == 0 ? from_left : SA[w - 1][TPT - 1], SA[w][TPT - 1], 0x5432);
+    for (int w = 0; w < WA; ++w) {
+      const uint32_t prev = w == 0 ? from_left : SA[w - 1][TPT - 1];
+      din[w] = PAIR ? prev : __byte_perm(prev, SA[w][TPT - 1], 0x5432);
+    }
     uint32_t pend = 0;
 #pragma unroll
     for (int w = 0; w < WA; ++w) {
@@ -517,8 +574,9 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       cur = window_of(a, t);
       if (cur.rows) break;
       if (gl == 0) {
-        a.out[t] = cur.res;
+        if (writeA) a.out[t] = cur.res;
         if constexpr (MODE == kBoth) a.out2[t] = cur.res;
+        if constexpr (PAIR) if (writeB) outB[t] = cur.res;
       }
       t = successor(t);
     }
@@ -534,6 +592,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
     return v;
+  };
+  auto finish_halves = [&](uint32_t best) -> uint32_t {   // per half (query-pair mode)
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) best = __vmaxs2(best, __shfl_xor_sync(gmask, best, o));
+    return best;
   };
   issue_grab();
   start_at(take_chunk());
@@ -553,7 +616,7 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
     for (int r = 0; r < R; ++r) {
       const int cl = class_of_row(r);
       if constexpr (DO_LIN) row_lin(cl);
-      if constexpr (MODE == kAff) row_aff(cl);
+      if constexpr (MODE == kAff || MODE == kPair) row_aff(cl);
       if constexpr (MODE == kBoth) row_aff(r == 0 && pad0 ? kClsPad : cl);
     }
     if (active) {
@@ -561,11 +624,16 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       if (cur.pos >= cur.end) {
         // target finished (rows past its end were padding rows)
         const int vl = DO_LIN ? finish(bestL) : 0;
-        const int va = DO_AFF ? finish(bestA) : 0;
+        const int va = (DO_AFF && !PAIR) ? finish(bestA) : 0;
+        const uint32_t vp = PAIR ? finish_halves(bestA) : 0u;
         if (gl == 0) {
           if constexpr (MODE == kLin) a.out[t] = vl;
           if constexpr (MODE == kAff) a.out[t] = va;
           if constexpr (MODE == kBoth) { a.out[t] = vl; a.out2[t] = va; }
+          if constexpr (PAIR) {
+            if (writeA) a.out[t] = (int)(int16_t)(vp & 0xffffu);
+            if (writeB) outB[t] = (int)(int16_t)(vp >> 16);
+          }
         }
         reset();
         if (pf_nxt) {
@@ -608,7 +676,7 @@ KernelInfo make_info() {
   constexpr int W = words_for<TPT, WIDE, MODE>();
   KernelInfo k;
   k.fn = sw_stream_kernel<TPT, W, MODE>;
-  using L = Layout<TPT, W, vector_major<TPT, W, MODE>()>;
+  using L = Layout<TPT, W, vector_major<TPT, W, MODE>(), MODE == kPair>;
   k.smem = L::smem + (MODE == kBoth ? L::smem - 256 : 0);
   k.threads = Shape<TPT, W, MODE>::threads;
   k.groups_per_block = (k.threads / 32) * L::GPW;
@@ -625,7 +693,7 @@ KernelInfo make_info() {
 // registers there, which leaves 8 warps per SM.
 constexpr int kMaxFusedTpt = 21;
 struct Tables {
-  KernelInfo k[2][3][64];
+  KernelInfo k[2][kModes][64];
 };
 
 template <int T, bool WIDE>
@@ -633,6 +701,7 @@ void fill_one(Tables& t) {
   t.k[WIDE][kLin][T - 1] = make_info<T, kLin, WIDE>();
   t.k[WIDE][kAff][T - 1] = make_info<T, kAff, WIDE>();
   if constexpr (T <= kMaxFusedTpt) t.k[WIDE][kBoth][T - 1] = make_info<T, kBoth, WIDE>();
+  t.k[WIDE][kPair][T - 1] = make_info<T, kPair, WIDE>();
 }
 
 template <int LO, bool WIDE, int... I>

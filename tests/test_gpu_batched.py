@@ -29,10 +29,21 @@ def _pack(queries):
     return enc, buf, lens
 
 
+@pytest.fixture(params=[False, True], ids=["one_per_row", "pairs"])
+def pairing(request):
+    """Run a test with the query-pair kernel off, then on, at every width."""
+    from sseqs_b200 import tune
+    before = [tune.get_query_pairing(t) for t in range(1, 65)]
+    tune.set_query_pairing(0, request.param)
+    yield request.param
+    for t, on in enumerate(before, 1):
+        tune.set_query_pairing(t, on)
+
+
 @pytest.mark.parametrize("lengths", [[300, 289, 320, 300, 305], [40, 33, 64], [2048, 2017],
                                      [7, 1, 32, 20]])
 @pytest.mark.parametrize("affine", [False, True])
-def test_scan_queries_equals_single_query_scans(lengths, affine):
+def test_scan_queries_equals_single_query_scans(lengths, affine, pairing):
     from sseqs_b200 import batched, dbtools
     sw = importlib.import_module("sseqs_b200.sw")
     _, db = _db()
@@ -60,7 +71,7 @@ def test_scan_queries_equals_single_query_scans(lengths, affine):
         assert torch.equal(got_2[i, :257], exp_2), i
 
 
-def test_length_outside_the_launch_width_is_not_scored():
+def test_length_outside_the_launch_width_is_not_scored(pairing):
     from sseqs_b200 import batched, dbtools
     _, db = _db()
     b = db.batches[0]
@@ -91,7 +102,7 @@ def _per_query_topk(db, enc, k):
 
 
 @pytest.mark.parametrize("use_graphs", [True, False])
-def test_search_queries_matches_per_query_topk(use_graphs):
+def test_search_queries_matches_per_query_topk(use_graphs, pairing):
     from sseqs_b200 import batched, dbtools
     _, db = _db()
     rng = np.random.default_rng(11)
@@ -107,3 +118,38 @@ def test_search_queries_matches_per_query_topk(use_graphs):
         mine = list(zip((-h.scores.astype(np.int64)).tolist(), h.batch.tolist(),
                         h.segment.tolist()))
         assert mine == exp, i
+
+
+PAIR_LENGTHS = [1, 17, 33, 64, 65, 100, 129, 200, 257, 300, 416, 500, 545, 640, 700, 858, 929,
+                1000, 1024, 1100, 1500, 1800, 2048]
+
+
+@pytest.mark.parametrize("L", PAIR_LENGTHS)
+def test_query_pairs_equal_unpaired_launches(L):
+    """Affine queries that share their targets are scored two per launch row
+    (query 2y in the low, 2y + 1 in the high half of every word); the scores
+    equal the one-query-per-row launch in both lane layouts, with an odd
+    query count and with one half of a pair outside the launch width."""
+    from sseqs_b200 import batched, dbtools, tune
+    _, db = _db()
+    b = db.batches[0]
+    tpt = (L + 31) // 32
+    lengths = [L, max(32 * (tpt - 1) + 1, L - 7), L, 32 * tpt, max(32 * (tpt - 1) + 1, L - 3)]
+    queries = [dbtools.random_query(x, 900 + i) for i, x in enumerate(lengths)]
+    enc, buf, lens = _pack(queries)
+    lens[3] = 32 * tpt + 1             # another width: not scored in either form
+    n = b.n_segments - 2
+    kw = dict(affine=True, g0=1, n_targets=n, skip=1, gap_a=11, gap_b=1)
+    before = tune.get_variant(3, tpt), tune.get_query_pairing(tpt)
+    try:
+        tune.set_query_pairing(tpt, False)
+        ref = batched.sw_scan_queries(buf, lens, tpt, b.ascii, b.delim, **kw)
+        tune.set_query_pairing(tpt, True)
+        for wide in (0, 1):
+            tune.set_variant(3, tpt, wide)
+            got = batched.sw_scan_queries(buf, lens, tpt, b.ascii, b.delim, **kw)
+            assert torch.equal(got[:, :n], ref[:, :n]), wide
+    finally:
+        tune.set_variant(3, tpt, before[0])
+        tune.set_query_pairing(tpt, before[1])
+    assert bool((ref[3, :n] == torch.iinfo(torch.int32).min).all())

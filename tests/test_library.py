@@ -90,8 +90,11 @@ def test_score_kernel_registry_matches_dispatch_rules(built_lib):
         assert tune.has_wide(1, t) == (2 <= t <= 16), t
         if t <= 21:
             assert tune.has_wide(2, t) == (2 <= t <= 16), t
+        # the query-pair kernel (mode 3) exists at every width, with the
+        # affine kernel's layouts
+        assert words(3, t, 0) == words(1, t, 0) and words(3, t, 1) == words(1, t, 1), t
     assert words(0, 27, 1) == 2 and words(0, 27, 0) == 1
-    assert L.sseqs_sw_variant_words(3, 5, 0) == -1 and L.sseqs_sw_variant_words(0, 65, 0) == -1
+    assert L.sseqs_sw_variant_words(4, 5, 0) == -1 and L.sseqs_sw_variant_words(0, 65, 0) == -1
 
 
 def test_variant_selection_round_trips(built_lib):
@@ -106,7 +109,7 @@ def test_variant_selection_round_trips(built_lib):
     finally:
         tune.set_variant(1, 9, before)
     L = built_lib
-    assert L.sseqs_sw_get_variant(3, 1) == -1 and L.sseqs_sw_get_variant(0, 65) == -1
+    assert L.sseqs_sw_get_variant(4, 1) == -1 and L.sseqs_sw_get_variant(0, 65) == -1
 
 
 def test_scan_both_argument_checks_without_a_gpu(built_lib):
