@@ -25,8 +25,10 @@
 // every (query, row) whose score reaches the query's threshold to that
 // query's candidate list -- the [queries x database] score matrix is never
 // written.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <climits>
@@ -544,6 +546,271 @@ __global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int*
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_BN));
 }
 
+// ------------------------------------------- tcgen05 GEMM, TMA-fed, persistent
+// The same N = 256 GEMMs, warp-specialised: warp 0 (one thread) loads the
+// tiles with TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast:
+// operands are this GPU's own memory), warp 1 (one thread) issues the MMAs,
+// warps 2-9 drain the accumulators.  Four stages of A (128 x 64 bf16) and B
+// (256 x 64) -- 192 KB -- and two 128 x 256 fp32 accumulators in tensor
+// memory (all 512 columns), so the epilogue of one M tile runs while the
+// next accumulates.  CTAs are persistent (one per SM) and take M tiles in
+// turn.  Barriers: full[s] (TMA bytes landed), empty[s] (the MMAs that read
+// stage s are done), acc_full[b] (accumulator b complete), acc_empty[b]
+// (its 8 epilogue warps have read it).  Every wait is bounded; one that runs
+// out sets *err, raises the CTA's abort flag and the roles stop issuing work;
+// before the tensor memory is freed the MMA thread waits (bounded) for its
+// last MMAs and the loader for its outstanding loads.
+//
+// A may be an overlapping row view (the conv GEMMs: row m of im2col(Y) starts
+// lda elements after row m-1 and spans K = 5 * lda): its tensor map is the
+// 2D array of lda-wide rows, and the K tile at k0 is the box at column
+// k0 % lda of row m0 + k0 / lda (a tile never crosses a row when lda % 64 ==
+// 0; for lda >= K it is the plain matrix).
+constexpr int WS_STAGES = 4, WS_EPI_WARPS = 8, WS_THREADS = 32 * (2 + WS_EPI_WARPS);
+constexpr size_t WS_SMEM = (size_t)WS_STAGES * TC_STAGE_BYTES + 1024;
+
+// Shared-memory matrix descriptor, K-major with the 128-byte swizzle: rows of
+// 128 bytes (64 bf16 of K), 8-row swizzle atoms 1024 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                  // leading byte offset (unused for this layout)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 46;                  // version
+  d |= (uint64_t)2 << 61;                  // layout: 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];"
+      :: "r"(dst), "l"(map), "r"(x), "r"(y), "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(mbar) : "memory");
+}
+
+// Fused epilogue of one row's 32 accumulator columns c0 .. c0 + 31.
+template <int EPI>
+__device__ __forceinline__ void epi_store32(const GemmArgs& g, int64_t m, bool keep, int c0,
+                                            const uint32_t (&v)[32]) {
+  __align__(16) __nv_bfloat16 rs[32], ax[32];
+  if (EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+    const uint4* src = reinterpret_cast<const uint4*>(g.res + m * g.ldc + c0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(rs)[q] = src[q];
+  }
+  if (EPI == EPI_GELU_GRAD || EPI == EPI_GELU_GRAD_RES) {
+    const uint4* src = reinterpret_cast<const uint4*>(g.aux + m * g.ldc + c0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(ax)[q] = src[q];
+  }
+  __align__(16) __nv_bfloat16 outc[32], outz[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int64_t n = c0 + j;
+    const float acc = __uint_as_float(v[j]);
+    float cval = 0.f, zval = 0.f;
+    if (EPI == EPI_BF16) {
+      cval = keep ? acc : 0.f;
+    } else if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES) {
+      const __nv_bfloat16 zb = __float2bfloat16_rn(keep ? acc + g.bias[n] : 0.f);
+      zval = __bfloat162float(zb);
+      const float r = (EPI == EPI_BIAS_GELU_RES) ? __bfloat162float(rs[j]) : 0.f;
+      cval = keep ? gelu_f(zval) + r : 0.f;
+    } else if (EPI == EPI_GELU_GRAD) {
+      cval = keep ? acc * gelu_grad(__bfloat162float(ax[j])) : 0.f;
+    } else {   // EPI_GELU_GRAD_RES
+      const __nv_bfloat16 gb = __float2bfloat16_rn(keep ? acc + __bfloat162float(rs[j]) : 0.f);
+      zval = __bfloat162float(gb);
+      cval = keep ? zval * gelu_grad(__bfloat162float(ax[j])) : 0.f;
+    }
+    outc[j] = __float2bfloat16_rn(cval);
+    outz[j] = __float2bfloat16_rn(zval);
+  }
+  uint4* dc = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(g.C) + m * g.ldc + c0);
+  const uint4* sc = reinterpret_cast<const uint4*>(outc);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) dc[q] = sc[q];
+  if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+    uint4* dz = reinterpret_cast<uint4*>(g.C2 + m * g.ldc + c0);
+    const uint4* sz = reinterpret_cast<const uint4*>(outz);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dz[q] = sz[q];
+  }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+    gemm_ws_kernel(const __grid_constant__ CUtensorMap map_a,
+                   const __grid_constant__ CUtensorMap map_b, GemmArgs g, int a_row_len,
+                   int* err) {
+  extern __shared__ __align__(1024) unsigned char wsm[];
+  const uint32_t raw = smem_u32(wsm);
+  unsigned char* tiles = wsm + ((1024 - (raw & 1023)) & 1023);
+  __shared__ __align__(8) uint64_t full[WS_STAGES], empty[WS_STAGES];
+  __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], mma_done;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ volatile int abort_s;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t ntiles = (g.M + TC_BM - 1) / TC_BM;
+  const int ktiles = (int)(g.K / TC_BK);
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base_s)), "r"(2 * TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < WS_STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&full[s])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&empty[s])), "r"(1));
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&acc_full[b])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                   :: "r"(smem_u32(&acc_empty[b])), "r"(WS_EPI_WARPS));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mma_done)), "r"(1));
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+  auto fail = [&]() {
+    abort_s = 1;
+    atomicExch(err, 1);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ loader
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" :: "l"(&map_a) : "memory");
+      asm volatile("prefetch.tensormap [%0];" :: "l"(&map_b) : "memory");
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t loads[WS_STAGES] = {};      // loads issued into each stage
+      for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+        const int m0 = (int)(t * TC_BM);
+        for (int kt = 0; kt < ktiles && !abort_s; ++kt) {
+          if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1)) { fail(); break; }
+          const uint32_t fb = smem_u32(&full[stage]);
+          mbar_expect_tx(fb, (uint32_t)TC_STAGE_BYTES);
+          const uint32_t a = smem_u32(tiles + stage * TC_STAGE_BYTES);
+          const int k0 = kt * TC_BK;
+          tma_load_2d(a, &map_a, k0 % a_row_len, m0 + k0 / a_row_len, fb);
+          tma_load_2d(a + TC_A_BYTES, &map_b, k0, 0, fb);
+          ++loads[stage];
+          if (++stage == WS_STAGES) { stage = 0; phase ^= 1; }
+        }
+      }
+      // before exit every issued load has landed: on the normal path the
+      // MMAs consumed them all; after an abort, wait (bounded) for the last
+      // load of each stage, which completes phase loads - 1 of its barrier
+      if (abort_s) {
+        for (int s2 = 0; s2 < WS_STAGES; ++s2)
+          if (loads[s2] > 0) mbar_wait(smem_u32(&full[s2]), (loads[s2] - 1) & 1u);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issue
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int b = 0;
+      uint32_t acc_phase = 0;
+      bool any = false;
+      for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+        if (!mbar_wait(smem_u32(&acc_empty[b]), acc_phase ^ 1)) { fail(); break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * TC_BN);
+        for (int kt = 0; kt < ktiles; ++kt) {
+          if (!mbar_wait(smem_u32(&full[stage]), phase)) { fail(); break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(tiles + stage * TC_STAGE_BYTES);
+          const uint32_t b0 = a0 + TC_A_BYTES;
+#pragma unroll
+          for (int ks = 0; ks < TC_BK / 16; ++ks) {
+            const uint64_t da = umma_desc_sw128(a0 + ks * 32);
+            const uint64_t db = umma_desc_sw128(b0 + ks * 32);
+            const uint32_t accum = (kt > 0 || ks > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                :: "r"(acc), "l"(da), "l"(db), "r"(kIdescBf16), "r"(accum));
+          }
+          any = true;
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                       :: "r"(smem_u32(&empty[stage])) : "memory");
+          if (++stage == WS_STAGES) { stage = 0; phase ^= 1; }
+        }
+        if (abort_s) break;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&acc_full[b])) : "memory");
+        if (++b == 2) { b = 0; acc_phase ^= 1; }
+      }
+      // every MMA issued is complete before the tensor memory is freed
+      if (any) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&mma_done)) : "memory");
+        if (!mbar_wait(smem_u32(&mma_done), 0)) fail();
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int e = warp - 2;
+    const int q = warp & 3;                      // tensor-memory lanes 32q .. 32q + 31
+    const int cbeg = (e >> 2) * (TC_BN / 2);     // columns [cbeg, cbeg + 128)
+    int b = 0;
+    uint32_t acc_phase = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+      if (!mbar_wait(smem_u32(&acc_full[b]), acc_phase)) { if (lane == 0) fail(); break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int64_t m = t * TC_BM + q * 32 + lane;
+      const bool row_ok = m < g.M;
+      const bool keep = row_ok && (g.row_mask ? g.row_mask[m] != 0 : true);
+#pragma unroll 1
+      for (int c0 = cbeg; c0 < cbeg + TC_BN / 2; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TC_BN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+            "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+              "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+              "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row_ok) epi_store32<EPI>(g, m, keep, c0, v);
+      }
+      // this warp has read accumulator b: hand it back to the MMA thread
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+      if (++b == 2) { b = 0; acc_phase ^= 1; }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(2 * TC_BN));
+}
+
 // ------------------------------------------------------------ elementwise
 // X0[p][c] = E[cls[p]][c] for real rows (cls < 21), 0 for padding (cls 255).
 __global__ void embed_lookup_kernel(const uint8_t* cls, int64_t P, const __nv_bfloat16* E, int D,
@@ -987,6 +1254,60 @@ int launch_tc(const GemmArgs& g, cudaStream_t stream) {
   return status_of(cudaGetLastError());
 }
 
+// Tensor map of a row-major bf16 array of `rows` rows of `row_len`
+// elements (row stride ld elements), boxes of 64 x box_rows, 128-byte swizzle;
+// rows past the end read as zero.
+static bool make_map(CUtensorMap* map, const void* base, int64_t row_len, int64_t rows,
+                     int64_t ld, int box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)row_len, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// The TMA-fed kernel applies when the operands' K tiles are boxes: A with
+// lda >= K (a plain matrix) or lda % 64 == 0 (an overlapping row view), B
+// with ldb >= K; 16-byte aligned bases and strides (checked by the caller).
+static bool ws_applies(const GemmArgs& g) {
+  return (g.lda >= g.K || g.lda % TC_BK == 0) && g.ldb >= g.K && g.lda <= INT32_MAX &&
+         g.M + g.K / std::max<int64_t>(1, g.lda) < INT32_MAX;
+}
+
+template <int EPI>
+int launch_tc_ws(const GemmArgs& g, cudaStream_t stream) {
+  int* err = tc_err_ptr();
+  if (!err) return SSEQS_ERR_CUDA;
+  // A: lda-wide rows (the K tile at k0 is column k0 % lda of row m + k0 / lda)
+  const int64_t a_len = g.lda >= g.K ? g.K : g.lda;
+  const int64_t a_rows = g.M + (g.lda >= g.K ? 0 : (g.K - 1) / g.lda);
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, g.A, a_len, a_rows, g.lda, TC_BM) ||
+      !make_map(&mb, g.B, g.K, TC_BN, g.ldb, TC_BN))
+    return SSEQS_ERR_CUDA;
+  auto fn = gemm_ws_kernel<EPI>;
+  if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)WS_SMEM) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const int64_t ntiles = (g.M + TC_BM - 1) / TC_BM;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, device_sm_count()));
+  const int row_len = (int)(g.lda >= g.K ? (g.K + TC_BK) : g.lda);   // > every k0 when plain
+  { fn<<<grid, WS_THREADS, WS_SMEM, stream>>>(ma, mb, g, row_len, err); count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
 // 1 = use the tcgen05 kernel where it applies (default), 0 = mma.sync only.
 extern "C" int sseqs_gemm_set_tensor_path(int tcgen05) {
   g_tc_enabled = tcgen05 != 0;
@@ -1042,6 +1363,15 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
       (!res || (reinterpret_cast<uintptr_t>(res) & 15) == 0) &&
       (!aux || (reinterpret_cast<uintptr_t>(aux) & 15) == 0) &&
       epilogue != EPI_F32 && epilogue != EPI_F32_ADD) {
+    if (ws_applies(g)) {
+      switch (epilogue) {
+        case EPI_BF16: return launch_tc_ws<EPI_BF16>(g, stream);
+        case EPI_BIAS_GELU: return launch_tc_ws<EPI_BIAS_GELU>(g, stream);
+        case EPI_GELU_GRAD: return launch_tc_ws<EPI_GELU_GRAD>(g, stream);
+        case EPI_BIAS_GELU_RES: return launch_tc_ws<EPI_BIAS_GELU_RES>(g, stream);
+        case EPI_GELU_GRAD_RES: return launch_tc_ws<EPI_GELU_GRAD_RES>(g, stream);
+      }
+    }
     switch (epilogue) {
       case EPI_BF16: return launch_tc<EPI_BF16>(g, stream);
       case EPI_BIAS_GELU: return launch_tc<EPI_BIAS_GELU>(g, stream);

@@ -109,6 +109,36 @@ def test_tcgen05_gemm_matches_mma_sync_and_fp32(M, epi, K):
     assert (outs[0][0] - outs[1][0]).abs().max().item() <= 2e-2 * scale
 
 
+@pytest.mark.parametrize("M", [5, 128, 1000, 40000])
+def test_tcgen05_gemm_overlapping_rows(M):
+    """The conv form: row m of A starts lda = 256 elements after row m - 1
+    and spans K = 5 * 256 (im2col without a buffer); the TMA-fed tcgen05
+    kernel loads each K tile as a box of the lda-wide rows.  Same result as
+    the mma.sync kernel and an fp32 reference."""
+    from sseqs_b200 import _lib, learned
+    g = torch.Generator(device="cpu")
+    g.manual_seed(M)
+    C_, K, N = 256, 1280, 256
+    X = _bf(torch.randn(M + 4, C_, generator=g)).cuda()
+    B = _bf(torch.randn(N, K, generator=g)).cuda()
+    outs = []
+    for path in (1, 0):
+        _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(path), "path")
+        C = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda")
+        learned._gemm(0, 0, 1, M, N, K, X.data_ptr(), C_, B.data_ptr(), K, C.data_ptr(), N,
+                      0, None, 0, None, 0)
+        torch.cuda.synchronize()
+        outs.append(C.float())
+    _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(1), "path")
+    assert _gemm_error() == 0
+    A = X.float().unfold(0, 5, 1).permute(0, 2, 1).reshape(M, K)    # row m = X[m .. m+4]
+    ref = A @ B.float().T
+    scale = max(1.0, ref.abs().max().item())
+    for C in outs:
+        assert (C - ref).abs().max().item() <= 2e-2 * scale
+    assert (outs[0] - outs[1]).abs().max().item() <= 2e-2 * scale
+
+
 @pytest.mark.parametrize("M,N,K", [(160, 256, 96), (1280, 256, 4096), (40, 24, 32)])
 def test_gemm_tn_matches_fp32(M, N, K):
     from sseqs_b200 import learned
