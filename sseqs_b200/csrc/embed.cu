@@ -52,13 +52,20 @@ enum Epi : int {
   EPI_GELU_GRAD_RES = 6,  // G = acc + res -> C2 (bf16), C = G * gelu'(aux); masked rows -> 0
 };
 
+// tanh by the hardware approximation (one MUFU instruction, relative error
+// about 2^-11): GELU's outputs are rounded to bf16 (2^-8) right after.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu_f(float z) {
   const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
-  return 0.5f * z * (1.f + tanhf(u));
+  return 0.5f * z * (1.f + tanh_fast(u));
 }
 __device__ __forceinline__ float gelu_grad(float z) {
   const float u = 0.7978845608f * (z + 0.044715f * z * z * z);
-  const float t = tanhf(u);
+  const float t = tanh_fast(u);
   return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * 0.7978845608f * (1.f + 0.134145f * z * z);
 }
 
