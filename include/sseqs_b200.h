@@ -339,6 +339,14 @@ int sseqs_gemm_error(int* out);
  * untouched). */
 int sseqs_embed_layout(const uint8_t* ascii, const int64_t* off, const int32_t* len,
                        const int64_t* row0, int n_seqs, uint8_t* cls, cudaStream_t stream);
+/* The first convolution of the embedder from a table: Z[p] = bf16(bias +
+ * sum_{t<5} T[t][cls[p-2+t]]) (fp32 T [5][21][D]: T[t][k] = E[k] . W1[:, t, :]^T;
+ * rows outside 0..P-1 and padding classes add nothing), Y[p] = bf16(GELU(Z[p]));
+ * rows with row_mask 0 are 0 in both; Z nullable.  Y, Z bf16 [P x D] with row
+ * stride D, D % 8 == 0, D <= 512.  No reference counterpart. */
+int sseqs_embed_conv1_table(const uint8_t* cls, int64_t P, const float* T, const float* bias,
+                            const uint8_t* row_mask, int D, void* Y, void* Z,
+                            cudaStream_t stream);
 /* X[p][c] = E[cls[p]][c] (bf16, E [21][D]); 0 for padding rows. */
 int sseqs_embed_lookup(const uint8_t* cls, int64_t P, const void* E, int D, void* X,
                        cudaStream_t stream);

@@ -60,6 +60,7 @@ _SIGNATURES = {
     "sseqs_gemm_error": (_I, [ctypes.POINTER(_I)]),
     "sseqs_embed_layout": (_I, [_P, _P, _P, _P, _I, _P, _P]),
     "sseqs_embed_lookup": (_I, [_P, _I64, _P, _I, _P, _P]),
+    "sseqs_embed_conv1_table": (_I, [_P, _I64, _P, _P, _P, _I, _P, _P, _P]),
     "sseqs_embed_grad": (_I, [_P, _I64, _P, _I, _P, _P]),
     "sseqs_pool_normalize": (_I, [_P, _I, _P, _P, _I, _P, _P, _P, _P]),
     "sseqs_pair_loss": (_I, [_P, _I, _P, _P, _P, _P, _I64, _P, _P, _P, _P]),

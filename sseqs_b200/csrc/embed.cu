@@ -261,10 +261,10 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(GemmArgs g) {
             r0 = __bfloat162float(rs[0]);
             r1 = two ? __bfloat162float(rs[1]) : 0.f;
           }
-          z[0] = zb0;
+          if (g.C2) z[0] = zb0;
           c[0] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb0)) + r0 : 0.f);
           if (two) {
-            z[1] = zb1;
+            if (g.C2) z[1] = zb1;
             c[1] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zb1)) + r1 : 0.f);
           }
         } else if (EPI == EPI_GELU_GRAD_RES) {
@@ -304,11 +304,27 @@ int launch_gemm(const GemmArgs& g, cudaStream_t stream, int splits = 1) {
   if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return SSEQS_ERR_CUDA;
-  const dim3 grid((unsigned)((g.N + BN - 1) / BN), (unsigned)((g.M + BM - 1) / BM),
-                  (unsigned)splits);
-  if (grid.y > 65535u || grid.z > 65535u) return SSEQS_ERR_UNSUPPORTED;
-  { fn<<<grid, GEMM_THREADS, smem, stream>>>(g); count_launches(1); }
-  return status_of(cudaGetLastError());
+  if (splits > 65535) return SSEQS_ERR_UNSUPPORTED;
+  // blockIdx.y counts M tiles, at most 65535 per launch: longer M runs as
+  // several launches over row ranges (the operands and outputs offset)
+  constexpr int64_t kRows = (int64_t)65535 * BM;
+  constexpr int64_t c_elem = (EPI == EPI_F32 || EPI == EPI_F32_ADD) ? 4 : 2;
+  for (int64_t m0 = 0; m0 < g.M; m0 += kRows) {
+    GemmArgs p = g;
+    p.M = std::min(kRows, g.M - m0);
+    p.A = A_T ? g.A + m0 : g.A + m0 * g.lda;
+    p.C = static_cast<char*>(g.C) + m0 * g.ldc * c_elem;
+    if (g.C2) p.C2 = g.C2 + m0 * g.ldc;
+    if (g.aux) p.aux = g.aux + m0 * g.ldc;
+    if (g.res) p.res = g.res + m0 * g.ldc;
+    if (g.row_mask) p.row_mask = g.row_mask + m0;
+    const dim3 grid((unsigned)((p.N + BN - 1) / BN), (unsigned)((p.M + BM - 1) / BM),
+                    (unsigned)splits);
+    { fn<<<grid, GEMM_THREADS, smem, stream>>>(p); count_launches(1); }
+    const int st = status_of(cudaGetLastError());
+    if (st != SSEQS_OK) return st;
+  }
+  return SSEQS_OK;
 }
 
 // ------------------------------------------------------- tcgen05 GEMM
@@ -539,7 +555,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int*
       const uint4* sc = reinterpret_cast<const uint4*>(outc);
 #pragma unroll
       for (int q = 0; q < 4; ++q) dc[q] = sc[q];
-      if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+      if ((EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) && g.C2) {
         uint4* dz = reinterpret_cast<uint4*>(g.C2 + m * g.ldc + c0);
         const uint4* sz = reinterpret_cast<const uint4*>(outz);
 #pragma unroll
@@ -647,7 +663,9 @@ __device__ __forceinline__ void epi_store32(const GemmArgs& g, int64_t m, bool k
   const uint4* sc = reinterpret_cast<const uint4*>(outc);
 #pragma unroll
   for (int q = 0; q < 4; ++q) dc[q] = sc[q];
-  if (EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) {
+  // the pre-activation (C2) is optional for the forward epilogues: only the
+  // backward pass reads it
+  if ((EPI == EPI_BIAS_GELU || EPI == EPI_BIAS_GELU_RES || EPI == EPI_GELU_GRAD_RES) && g.C2) {
     uint4* dz = reinterpret_cast<uint4*>(g.C2 + m * g.ldc + c0);
     const uint4* sz = reinterpret_cast<const uint4*>(outz);
 #pragma unroll
@@ -819,6 +837,53 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
 }
 
 // ------------------------------------------------------------ elementwise
+// First convolution as a table.  Its input rows are class embeddings, so
+// the pre-activation of row p is b + sum_t T[t][cls[p-2+t]] with
+// T[t][k] = E[k] . W1[:, t, :]^T (rows outside the layout and padding rows
+// contribute nothing): a gather-add of five 256-wide rows instead of a K = 160
+// GEMM.  Same epilogue as EPI_BIAS_GELU: Z = bf16(z), Y = GELU(Z); masked
+// rows 0; Z optional.  A thread writes 8 channels of one row; T in shared
+// memory (5 x 21 x D fp32).
+__global__ void conv1_table_kernel(const uint8_t* cls, int64_t P, const float* T,
+                                   const float* bias, const uint8_t* mask, int D,
+                                   __nv_bfloat16* Y, __nv_bfloat16* Z) {
+  extern __shared__ float4 t_sm[];
+  float* Ts = reinterpret_cast<float*>(t_sm);
+  for (int i = threadIdx.x; i < 5 * 21 * D / 4; i += blockDim.x)
+    t_sm[i] = reinterpret_cast<const float4*>(T)[i];
+  __syncthreads();
+  const int per_row = D / 8;
+  const int64_t total = P * per_row;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / per_row;
+    const int c0 = (int)(i - p * per_row) * 8;
+    const bool keep = mask ? mask[p] != 0 : true;
+    float z[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) z[j] = bias[c0 + j];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      const int64_t q = p - 2 + t;
+      const int k = (q >= 0 && q < P) ? cls[q] : 255;
+      if (k < 21) {
+        const float4* tr = reinterpret_cast<const float4*>(Ts + ((size_t)t * 21 + k) * D + c0);
+        const float4 a = tr[0], b = tr[1];
+        z[0] += a.x; z[1] += a.y; z[2] += a.z; z[3] += a.w;
+        z[4] += b.x; z[5] += b.y; z[6] += b.z; z[7] += b.w;
+      }
+    }
+    __align__(16) __nv_bfloat16 zy[8], yy[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      zy[j] = __float2bfloat16_rn(keep ? z[j] : 0.f);
+      yy[j] = __float2bfloat16_rn(keep ? gelu_f(__bfloat162float(zy[j])) : 0.f);
+    }
+    *reinterpret_cast<uint4*>(Y + p * D + c0) = *reinterpret_cast<const uint4*>(yy);
+    if (Z) *reinterpret_cast<uint4*>(Z + p * D + c0) = *reinterpret_cast<const uint4*>(zy);
+  }
+}
+
 // X0[p][c] = E[cls[p]][c] for real rows (cls < 21), 0 for padding (cls 255).
 __global__ void embed_lookup_kernel(const uint8_t* cls, int64_t P, const __nv_bfloat16* E, int D,
                                     __nv_bfloat16* X) {
@@ -1344,9 +1409,9 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
   if (!al(A) || !al(B) || (lda % 8) != 0 || (ldb % 8) != 0) return SSEQS_ERR_ARG;
   if (a_t && (M % 8) != 0) return SSEQS_ERR_ARG;
   if (b_t && (N % 8) != 0) return SSEQS_ERR_ARG;
-  if (epilogue == EPI_BIAS_GELU && (!bias || !C2)) return SSEQS_ERR_ARG;
+  if (epilogue == EPI_BIAS_GELU && !bias) return SSEQS_ERR_ARG;
   if ((epilogue == EPI_GELU_GRAD || epilogue == EPI_GELU_GRAD_RES) && !aux) return SSEQS_ERR_ARG;
-  if ((epilogue == EPI_BIAS_GELU_RES && (!bias || !C2 || !res)) ||
+  if ((epilogue == EPI_BIAS_GELU_RES && (!bias || !res)) ||
       (epilogue == EPI_GELU_GRAD_RES && (!C2 || !res)))
     return SSEQS_ERR_ARG;
   if (epilogue < 0 || epilogue > 6) return SSEQS_ERR_ARG;
@@ -1401,6 +1466,28 @@ extern "C" int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_
     case 8 | 4 | 0: return launch_gemm<true, true, EPI_F32>(g, stream);
     default: return SSEQS_ERR_UNSUPPORTED;
   }
+}
+
+extern "C" int sseqs_embed_conv1_table(const uint8_t* cls, int64_t P, const float* T,
+                                       const float* bias, const uint8_t* row_mask, int D,
+                                       void* Y, void* Z, cudaStream_t stream) {
+  if (P < 0 || D <= 0 || D % 8 != 0 || D > 512) return SSEQS_ERR_ARG;
+  if (P == 0) return SSEQS_OK;
+  if (!cls || !T || !bias || !Y) return SSEQS_ERR_ARG;
+  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  if (!al(T) || !al(Y) || (Z && !al(Z))) return SSEQS_ERR_ARG;
+  const size_t smem = sizeof(float) * 5 * 21 * (size_t)D;
+  if (cudaFuncSetAttribute((const void*)conv1_table_kernel,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return SSEQS_ERR_CUDA;
+  const int64_t work = P * (D / 8);
+  const int grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>((work + 255) / 256, (int64_t)device_sm_count() * 4));
+  { conv1_table_kernel<<<grid, 256, smem, stream>>>(
+        cls, P, T, bias, row_mask, D, static_cast<__nv_bfloat16*>(Y),
+        static_cast<__nv_bfloat16*>(Z));
+    count_launches(1); }
+  return status_of(cudaGetLastError());
 }
 
 extern "C" int sseqs_embed_lookup(const uint8_t* cls, int64_t P, const void* E, int D, void* X,

@@ -65,14 +65,22 @@ class Layout:
         return self.start.numel()
 
 
+def layout_rows(lengths: torch.Tensor, max_len: int = MAX_LEN) -> torch.Tensor:
+    """Rows a layout of these sequences needs before rounding (device int64
+    scalar): 2 leading zero rows and each sequence's rows plus 2."""
+    return 2 + (lengths.to(torch.int64).clamp(0, max_len) + 2).sum()
+
+
 def make_layout(ascii: torch.Tensor, offsets: torch.Tensor, lengths: torch.Tensor,
-                max_len: int = MAX_LEN) -> Layout:
-    """Layout of the sequences ascii[offsets[s] : + lengths[s]] (device)."""
+                max_len: int = MAX_LEN, rows: int | None = None) -> Layout:
+    """Layout of the sequences ascii[offsets[s] : + lengths[s]] (device).
+    ``rows`` is ``layout_rows(lengths)`` when the caller knows it already
+    (which saves a device-to-host copy)."""
     dev = ascii.device
     L = lengths.to(torch.int64).clamp(0, max_len)
     sizes = L + 2
     row0 = torch.cumsum(sizes, 0) - sizes + 2
-    P = 2 + int(sizes.sum().item())
+    P = int(layout_rows(lengths, max_len).item()) if rows is None else int(rows)
     P = (P + 31) // 32 * 32
     cls = torch.full((P,), 255, dtype=torch.uint8, device=dev)
     n = L.numel()
@@ -90,9 +98,11 @@ class _Buffers:
     def __init__(self, rows: int, train: bool, dev):
         self.rows = rows
         z = lambda c: torch.zeros((rows + 4, c), dtype=torch.bfloat16, device=dev)
-        self.X0 = z(E)
-        self.Y = [z(D) for _ in range(4)]
-        self.Z = [z(D) for _ in range(4)] if train else [z(D)]
+        # inference keeps two layer outputs (alternating), no embedded rows
+        # and no pre-activations
+        self.X0 = z(E) if train else None
+        self.Y = [z(D) for _ in range(4 if train else 2)]
+        self.Z = [z(D) for _ in range(4)] if train else None
         self.dZ = [z(D) for _ in range(4)] if train else None
         self.G = [z(D) for _ in range(4)] if train else None
         self.dX0 = z(E) if train else None
@@ -134,6 +144,10 @@ class Embedder:
     def _sync_bf16(self):
         self.emb_b = self.emb.to(torch.bfloat16).contiguous()
         self.Wb = [w.reshape(D, -1).to(torch.bfloat16).contiguous() for w in self.W]
+        # the first convolution as a table: T[t][k] = E[k] . W1[:, t, :]^T from
+        # the same bf16 values the GEMM form would multiply
+        self.T1 = torch.einsum("kc,otc->tko", self.emb_b.float(),
+                               self.Wb[0].float().reshape(D, 5, E)).contiguous()
         self.Wf = [w.flip(1).permute(2, 1, 0).reshape(c, -1).to(torch.bfloat16).contiguous()
                    for w, c in zip(self.W, self.cin)]
 
@@ -161,18 +175,25 @@ class Embedder:
         bufs = self._buffers(lay.P, train)
         P = lay.P
         L = lib()
-        check(L.sseqs_embed_lookup(ptr(lay.cls), P, ptr(self.emb_b), E, _base(bufs.X0),
-                                   stream_ptr()), "embed_lookup")
-        prev, cprev = bufs.X0, E
-        for l in range(4):
-            Y = bufs.Y[l]
-            Z = bufs.Z[l] if train else bufs.Z[0]
+        if train:    # the backward pass reads the embedded rows
+            check(L.sseqs_embed_lookup(ptr(lay.cls), P, ptr(self.emb_b), E, _base(bufs.X0),
+                                       stream_ptr()), "embed_lookup")
+        # layer 1 from its table (a K = 160 GEMM otherwise); the pre-activations
+        # Z are kept for the backward pass only
+        check(L.sseqs_embed_conv1_table(ptr(lay.cls), P, ptr(self.T1), ptr(self.b[0]),
+                                        ptr(lay.mask), D, _base(bufs.Y[0]),
+                                        _base(bufs.Z[0]) if train else None, stream_ptr()),
+              "conv1_table")
+        prev = bufs.Y[0]
+        for l in range(1, 4):
+            Y = bufs.Y[l % len(bufs.Y)]
             # im2col(prev) row p starts at layout row p-2 = buffer row p
-            res = l > 0 and self.residual
-            _gemm(0, 0, _EPI_BIAS_GELU_RES if res else _EPI_BIAS_GELU, P, D, 5 * cprev,
-                  prev.data_ptr(), cprev, self.Wb[l].data_ptr(), 5 * cprev, _base(Y), D,
-                  _base(Z), self.b[l], None, lay.mask, _base(prev) if res else None)
-            prev, cprev = Y, D
+            res = self.residual
+            _gemm(0, 0, _EPI_BIAS_GELU_RES if res else _EPI_BIAS_GELU, P, D, 5 * D,
+                  prev.data_ptr(), D, self.Wb[l].data_ptr(), 5 * D, _base(Y), D,
+                  _base(bufs.Z[l]) if train else None, self.b[l], None, lay.mask,
+                  _base(prev) if res else None)
+            prev = Y
         S = lay.n
         pooled = torch.empty((S, D), dtype=torch.float32, device=self.device)
         emb = torch.empty((S, D), dtype=torch.float32, device=self.device)
@@ -250,12 +271,23 @@ class Embedder:
                                 self.emb.numel(), lr, b1, b2, eps, self.step, ptr(self.emb_b),
                                 st), "adam_flat")
 
-    def embed(self, ascii, offsets, lengths, chunk: int = 8192) -> torch.Tensor:
-        """Embeddings [n, 256] of many sequences, ``chunk`` at a time."""
+    def embed(self, ascii, offsets, lengths, chunk: int = 32768) -> torch.Tensor:
+        """Embeddings [n, 256] of many sequences, ``chunk`` at a time (the
+        row counts of all chunks come to the host in one copy, so the chunks
+        are queued without waiting for one another)."""
         n = lengths.numel()
         out = torch.empty((n, D), dtype=torch.float32, device=self.device)
-        for s in range(0, n, chunk):
-            lay = make_layout(ascii, offsets[s:s + chunk], lengths[s:s + chunk])
+        starts = list(range(0, n, chunk))
+        if not starts:
+            return out
+        L = lengths.to(torch.int64).clamp(0, MAX_LEN) + 2
+        bounds = torch.tensor(starts[1:] + [n], dtype=torch.int64, device=L.device)
+        cum = torch.cumsum(L, 0)
+        ends = cum[bounds - 1]
+        rows = to_host(2 + ends - torch.cat([torch.zeros(1, dtype=torch.int64, device=L.device),
+                                             ends[:-1]]))
+        for s, r in zip(starts, rows.tolist()):
+            lay = make_layout(ascii, offsets[s:s + chunk], lengths[s:s + chunk], rows=r)
             out[s:s + lay.n] = self.forward(lay)
         return out
 
@@ -446,7 +478,7 @@ def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
 class LearnedIndex:
     """FP8 codes of every database segment, resident in HBM."""
 
-    def __init__(self, model: Embedder, db, chunk: int = 8192):
+    def __init__(self, model: Embedder, db, chunk: int = 32768):
         self.model, self.db = model, db
         counts = [b.n_segments for b in db.batches]
         self.cum = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
@@ -454,13 +486,16 @@ class LearnedIndex:
         self.codes = torch.empty((max(n, 1), D), dtype=torch.uint8, device=db.device)
         L = lib()
         for bi, b in enumerate(db.batches):
-            for s in range(0, b.n_segments, chunk):
-                e = min(s + chunk, b.n_segments)
-                emb = model.embed(b.ascii, b.offsets[s:e], b.lengths[s:e], chunk=chunk)
-                row = int(self.cum[bi]) + s
-                check(L.sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE,
-                                            self.codes[row:row + (e - s)].data_ptr(),
-                                            stream_ptr()), "quantize")
+            if b.n_segments == 0:
+                continue
+            # a whole batch per call: its chunks are queued back to back
+            emb = model.embed(b.ascii, b.offsets[:b.n_segments], b.lengths[:b.n_segments],
+                              chunk=chunk)
+            row = int(self.cum[bi])
+            check(L.sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE,
+                                        self.codes[row:row + b.n_segments].data_ptr(),
+                                        stream_ptr()), "quantize")
+            del emb
         self.n = n
 
     def query_codes(self, enc_queries) -> torch.Tensor:
