@@ -471,6 +471,116 @@ def search_defaults_leg(M, db, queries):
             "settings": "bs=5e7, top_fft=200, top_sw=10, top_sw_affine=2, database resident"}
 
 
+SWEEP_RATES = (10, 50, 100, 250, 500)
+
+
+def serving_sweep(index, rates, seconds, seed=6, n_alone=4):
+    """The learned-prefilter request loop (``serve.SearchServer`` +
+    ``serve.LearnedExecutor``, continuous batching, up to 64 requests in
+    flight, admission by free device memory) under Poisson arrivals at each
+    rate for about ``seconds`` seconds (at least 20 requests), query lengths
+    U(50, 1000): served queries/s and latency percentiles per rate.  Then
+    ``n_alone`` requests of the last rate are scored again alone, and their
+    hits must equal the ones they got in the mix."""
+    import torch
+    from sseqs_b200 import dbtools, serve
+    ex = serve.LearnedExecutor(index, top_k=TOP_K)
+    free = (lambda: torch.cuda.mem_get_info()[0])
+    srv = serve.SearchServer(ex, top_k=TOP_K, max_slots=64, memory_reserve=2 << 30,
+                             free_memory=free)
+    rng = np.random.default_rng(seed)
+    srv.submit(dbtools.random_query(300, 1))                  # warm-up
+    while srv.step():
+        pass
+    srv.completed.clear()
+    out, last = [], None
+    srv.start()
+    try:
+        for rate in rates:
+            n = max(20, int(rate * seconds))
+            qs = [dbtools.random_query(int(L), 20000 + 997 * rate + i)
+                  for i, L in enumerate(rng.integers(50, 1001, n))]
+            offs = serve.poisson_arrivals(n, rate, seed=seed + rate)
+            steps0 = srv.steps
+            reqs = serve.replay(srv, qs, offs)
+            span = max(r.t_done for r in reqs) - min(r.t_submit for r in reqs)
+            st = serve.stats(reqs, span)
+            out.append({"arrival_rate_qps": rate, "requests": n,
+                        "queries_per_s": round(st.queries_per_s, 2),
+                        "p50_ms": round(st.p50_ms, 1), "p99_ms": round(st.p99_ms, 1),
+                        "mean_ms": round(st.mean_ms, 1), "engine_steps": srv.steps - steps0,
+                        "saturated": st.queries_per_s < 0.9 * rate})
+            last = reqs
+    finally:
+        srv.stop()
+    same = True
+    alone = serve.SearchServer(ex, top_k=TOP_K, max_slots=64)
+    for r in last[:n_alone]:
+        a = alone.submit(r.query)
+        while alone.step():
+            pass
+        ra, rb = a.result, r.result
+        same &= (np.array_equal(ra.scores, rb.scores) and np.array_equal(ra.batch, rb.batch)
+                 and np.array_equal(ra.segment, rb.segment))
+    return {"rates": out, "identical_alone_vs_mix": bool(same), "checked_alone": n_alone,
+            "pipeline": "learned prefilter (FP8 index, 32768 candidates) + exact affine SW, "
+                        "top-4096; up to 64 requests in flight",
+            "index_rows": index.n, "lengths": "U(50, 1000)"}
+
+
+def bench_serving_scale(args):
+    """``--serving-scale N``: a database of N synthetic sequences built in
+    shards of 20M (each with its own seed, decoded into the resident
+    database as it is made), the embedder trained as in the learned leg, the
+    FP8 index of every segment, and the serving sweep over it.  One JSON
+    line."""
+    import torch
+    from sseqs_b200 import dbtools, learned
+    from sseqs_b200.database import Database
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    queries = query_set()
+    db = Database([], bs=BS)
+    n_left, shard = int(args.serving_scale), 0
+    n_res = 0
+    while n_left > 0:
+        n = min(20_000_000, n_left)
+        syn = dbtools.synthetic_db(queries[:8], n, 0.0005, IDENT, seed=1000 + shard, device="cuda")
+        n_res += syn.n_residues
+        db.add_chunks(syn.chunks)
+        del syn
+        torch.cuda.empty_cache()
+        n_left -= n
+        shard += 1
+    t1 = time.time()
+    pairs = learned.training_pairs(max(1, args.learned_pairs // 256), 256, seed=5)
+    model = learned.Embedder(seed=5)
+    learned.train(model, pairs, epochs=args.learned_epochs, seed=5)
+    del pairs
+    torch.cuda.empty_cache()
+    t2 = time.time()
+    index = learned.LearnedIndex(model, db)
+    torch.cuda.synchronize()
+    t3 = time.time()
+    sweep = serving_sweep(index, SWEEP_RATES, args.sweep_seconds)
+    best = max(r["queries_per_s"] for r in sweep["rates"])
+    free, total = torch.cuda.mem_get_info()
+    out = {
+        "metric": "queries/s of the learned serving loop under Poisson arrivals (max over rates)",
+        "value": best, "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp8 e4m3 + int16x2",
+        "data": "synthetic",
+        "config": {"workload": "serving at the benchmark's serving scale",
+                   "db_sequences": int(args.serving_scale), "db_residues": int(n_res),
+                   "db_shards": shard, "index_bytes": int(index.codes.numel()),
+                   "device_bytes_in_use": int(total - free)},
+        "serving_sweep": sweep,
+        "seconds_build_db": round(t1 - t0, 1), "seconds_train": round(t2 - t1, 1),
+        "seconds_index": round(t3 - t2, 1),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def measured_peak(name):
     """sseqs_dpx_peak (ALU-pipe DPX issue rate) or sseqs_int16x2_peak (both
     int pipes), in int16x2 lane-instructions per second."""
@@ -708,6 +818,9 @@ def bench_b200(args):
             out["serving_learned"] = serving_leg(db, 4 * args.serve_requests,
                                                  args.serve_rate_learned,
                                                  index=learned_leg.index)
+        if args.sweep_seconds > 0:
+            out["serving_sweep"] = serving_sweep(learned_leg.index, SWEEP_RATES,
+                                                 args.sweep_seconds)
         learned_leg.index = None
     if world == 1 and not args.no_cpu_baseline:
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
@@ -826,11 +939,19 @@ def main():
                     help="queries timed in the learned-prefilter leg")
     ap.add_argument("--learned-epochs", type=int, default=2,
                     help="training epochs over the learned leg's pairs")
+    ap.add_argument("--sweep-seconds", type=float, default=4.0,
+                    help="seconds of Poisson arrivals per rate of the learned serving sweep "
+                         "(rates %s q/s); 0 skips it" % (SWEEP_RATES,))
+    ap.add_argument("--serving-scale", type=int, default=0,
+                    help="instead of the benchmark: build a database of this many sequences, "
+                         "its learned index, and run the serving sweep over it")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":
         bench_reference(args)
+    elif args.serving_scale > 0:
+        bench_serving_scale(args)
     else:
         bench_b200(args)
 

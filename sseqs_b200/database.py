@@ -72,15 +72,24 @@ class Database:
         self.packed = [] if keep_packed else None
         self.n_residues = 0
         self.index = None          # sidecar segment index (from_file), if any
-        for ci, ch in enumerate(chunks):
+        self.n_chunks = 0
+        self.add_chunks(chunks)
+
+    def add_chunks(self, chunks) -> None:
+        """Decode more packed chunks into resident batches (after the ones
+        already loaded), so a large database can be built a part at a time
+        without holding all of it packed."""
+        for ch in chunks:
+            ci = self.n_chunks
             ch = ch if isinstance(ch, torch.Tensor) else torch.from_numpy(np.asarray(ch, np.uint8))
             ch = ch.to(self.device, torch.uint8)
             if ch.numel() % self.bs:
                 raise ValueError("chunk size must be a multiple of bs (sseqs/msa.py:216)")
-            if keep_packed:
+            if self.packed is not None:
                 self.packed.append(ch)
             for j in range(ch.numel() // self.bs):
                 self._add_batch(ci, j, ch)
+            self.n_chunks += 1
             del ch
 
     def _add_batch(self, ci, j, ch):

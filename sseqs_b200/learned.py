@@ -568,30 +568,36 @@ class LearnedIndex:
         sw = importlib.import_module("sseqs_b200.sw")
         dev = self.db.device
         enc = [sw.encode_query(q, device=dev) for q in queries]
-        results = [[] for _ in queries]
-        per_batch = []
+        nb = len(self.db.batches)
+        # per query its candidate rows in order, and where each batch's
+        # scored segments (1 .. n-2) begin and end among them: one small
+        # device-to-host copy per query
+        bounds = torch.tensor([[int(self.cum[bi]) + 1, int(self.cum[bi]) + b.n_segments - 1]
+                               for bi, b in enumerate(self.db.batches)],
+                              dtype=torch.int64, device=dev).reshape(-1)
+        rows_sorted, cuts = [], []
         for c in cands:
             r = c.sort().values
-            cuts = torch.searchsorted(r, torch.tensor(self.cum, device=dev))
-            per_batch.append((r, cuts))
+            rows_sorted.append(r)
+            cuts.append(torch.searchsorted(r, bounds))
+        cuts = to_host(torch.stack(cuts)).reshape(len(cands), nb, 2) if cands else None
+        parts = [[] for _ in queries]          # (batch, segment ids, scores) on the device
         for bi, b in enumerate(self.db.batches):
-            lists = []
-            for qi, (r, cuts) in enumerate(per_batch):
-                f = r[int(cuts[bi]):int(cuts[bi + 1])] - int(self.cum[bi])
-                f = f[(f >= 1) & (f <= b.n_segments - 2)]
-                lists.append(f)
+            lists = [rows_sorted[qi][int(cuts[qi, bi, 0]):int(cuts[qi, bi, 1])] -
+                     int(self.cum[bi]) for qi in range(len(queries))]
             for tpt, members in batched.buckets([e.numel() for e in enc]).items():
-                for s in range(0, len(members), batched.GROUP):
-                    grp = [qi for qi in members[s:s + batched.GROUP] if lists[qi].numel()]
+                for s0 in range(0, len(members), batched.GROUP):
+                    grp = [qi for qi in members[s0:s0 + batched.GROUP] if lists[qi].numel()]
                     if not grp:
                         continue
                     m = max(lists[qi].numel() for qi in grp)
                     idx = torch.empty((len(grp), m), dtype=torch.int32, device=dev)
+                    segs = []
                     for j, qi in enumerate(grp):
-                        f = lists[qi]
-                        g = b.seg_index[f].to(torch.int32)
+                        g = b.seg_index[lists[qi]].to(torch.int32)
                         idx[j, :g.numel()] = g
                         idx[j, g.numel():] = g[-1]
+                        segs.append(g)
                     qbuf = torch.zeros((len(grp), batched.MAX_QUERY), dtype=torch.uint8,
                                        device=dev)
                     for j, qi in enumerate(grp):
@@ -602,20 +608,27 @@ class LearnedIndex:
                                                  good_idx=idx, skip=1, gap_a=gap_open,
                                                  gap_b=gap_extend)
                     for j, qi in enumerate(grp):
-                        n = lists[qi].numel()
-                        g = to_host(b.seg_index[lists[qi]].to(torch.int32))
-                        results[qi].append((bi, g, to_host(sc[j, :n]), b.maxlen))
+                        parts[qi].append((bi, segs[j], sc[j, :segs[j].numel()]))
+        # rank per query: normalised score desc, then batch, then segment
         out = []
         for qi, q in enumerate(queries):
-            rows = []
+            if not parts[qi]:
+                out.append([])
+                continue
             Lq = len(q)
-            for bi, f, s, maxlen in results[qi]:
-                norm = (s.astype(np.float32) / np.sqrt(np.float32(Lq * maxlen))).astype(
-                    np.float32)
-                for k in range(f.size):
-                    rows.append((float(norm[k]), bi, int(f[k]), int(s[k])))
-            rows.sort(key=lambda x: (-x[0], x[1], x[2]))
-            out.append(rows[:top])
+            seg = to_host(torch.cat([p[1] for p in parts[qi]])).astype(np.int64)
+            aff = to_host(torch.cat([p[2] for p in parts[qi]]))
+            bat = np.concatenate([np.full(p[1].numel(), p[0], np.int64) for p in parts[qi]])
+            mx = np.concatenate([np.full(p[1].numel(), self.db.batches[p[0]].maxlen, np.int64)
+                                 for p in parts[qi]])
+            norm = np.empty(aff.size, np.float32)
+            for ml in np.unique(mx):
+                sel = mx == ml
+                norm[sel] = (aff[sel].astype(np.float32) /
+                             np.sqrt(np.float32(Lq * int(ml)))).astype(np.float32)
+            keep = np.lexsort((seg, bat, -norm.astype(np.float64)))[:top]
+            out.append(list(zip(norm[keep].tolist(), bat[keep].tolist(), seg[keep].tolist(),
+                                aff[keep].astype(np.int64).tolist())))
         return out
 
     def search(self, queries, n_cand: int = 32768, top: int = 4096, **kw):
