@@ -528,6 +528,40 @@ def serving_sweep(index, rates, seconds, seed=6, n_alone=4):
             "index_rows": index.n, "lengths": "U(50, 1000)"}
 
 
+def exact_saturation(db, n_q=16, n_batches=3, seed=7):
+    """Saturation rate of the exact pipeline (``serve.GpuExecutor``: affine
+    SW of every segment, top-k per batch) at this database size: ``n_q``
+    requests of lengths U(50, 1000) scored together over the first
+    ``n_batches`` batches, timed with CUDA events, and the rate scaled to the
+    whole database by residues (the exact pipeline's cost is linear in
+    them)."""
+    import torch
+    from sseqs_b200 import dbtools, serve
+    ex = serve.GpuExecutor(db, top_k=TOP_K, max_slots=64)
+    rng = np.random.default_rng(seed)
+    reqs = [serve.Request(i, dbtools.random_query(int(L), 31000 + i), 0.0)
+            for i, L in enumerate(rng.integers(50, 1001, n_q))]
+    for r in reqs:
+        ex.prepare(r)
+    nb = min(n_batches, len(db.batches))
+    ex.step(0, reqs[:2])                                   # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for bi in range(nb):
+        ex.step(bi, reqs)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    res_sub = sum(b.n_residues for b in db.batches[:nb])
+    cells = sum(len(r.query) for r in reqs) * res_sub
+    whole = sec * db.n_residues / max(res_sub, 1)
+    return {"queries_per_s": round(n_q / whole, 4), "seconds_per_query": round(whole / n_q, 2),
+            "gcups": round(cells / sec / 1e9, 1), "queries": n_q,
+            "timed_batches": nb, "timed_residues": int(res_sub),
+            "note": "timed on the first batches, scaled to all residues"}
+
+
 def bench_serving_scale(args):
     """``--serving-scale N``: a database of N synthetic sequences built in
     shards of 20M (each with its own seed, decoded into the resident
@@ -563,6 +597,7 @@ def bench_serving_scale(args):
     torch.cuda.synchronize()
     t3 = time.time()
     sweep = serving_sweep(index, SWEEP_RATES, args.sweep_seconds)
+    sweep["exact_pipeline_saturation"] = exact_saturation(db)
     best = max(r["queries_per_s"] for r in sweep["rates"])
     free, total = torch.cuda.mem_get_info()
     out = {

@@ -385,11 +385,15 @@ int sseqs_adam_flat(float* w, float* m, float* v, const float* g, int64_t n, flo
 /* out[i] = e4m3 code of scale * x[i] (saturating). */
 int sseqs_quantize_e4m3(const float* x, int64_t n, float scale, uint8_t* out,
                         cudaStream_t stream);
-/* Candidate selection by FP8 GEMM (mma.sync e4m3, fp32 accumulation): for
- * every query q (codes Q [nq][256]) and database row r (codes DB [n][256])
- * with <Q[q], DB[r]> >= tau[q], appends r (and the dot product) to q's list:
+/* Candidate selection by FP8 GEMM (e4m3, fp32 accumulation): for every
+ * query q (codes Q [nq][256]) and database row r (codes DB [n][256]) with
+ * <Q[q], DB[r]> >= tau[q], appends r (and the dot product) to q's list:
  * slot = count[q]++ (count zeroed by the caller), kept when slot < cap, at
- * cand[q*cap + slot] / cand_score[q*cap + slot].  Q, DB 16-byte aligned. */
+ * cand[q*cap + slot] / cand_score[q*cap + slot]; list order is not fixed.
+ * Q, DB 16-byte aligned.  Runs on tcgen05.mma kind::f8f6f4 (database rows
+ * as M = 128, queries as N = nq rounded up to 16, at most 256 per tile, TMA
+ * loads) unless sseqs_gemm_set_tensor_path(0) selected mma.sync; a bounded
+ * wait that ran out sets the flag sseqs_gemm_error reads. */
 int sseqs_score_select(const uint8_t* Q, int nq, const uint8_t* DB, int64_t n, const float* tau,
                        int32_t* count, int64_t* cand, float* cand_score, int cap,
                        cudaStream_t stream);

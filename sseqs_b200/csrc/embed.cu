@@ -1246,6 +1246,203 @@ __global__ void __launch_bounds__(GEMM_THREADS) score_dense_kernel(SelArgs a, fl
     }
 }
 
+// ------------------------------------- FP8 score + select on tcgen05 (TMA)
+// The same selection as score_select_kernel with the database rows as the
+// M = 128 operand of tcgen05.mma kind::f8f6f4 and the query tile as N (the
+// batch rounded up to 16, at most 256, so a small batch does not pay for a
+// 128-query tile).  Persistent CTAs (one per SM) take 128-row database tiles
+// in turn; warp 0 loads them with TMA (two 128 x 128-byte boxes per tile,
+// 128-byte swizzle, no multicast: the codes are this GPU's own memory) into
+// SEL_STAGES_MAX stages at most, warp 1 issues the eight K = 32 MMAs of a
+// tile into one of two tensor-memory accumulators, and warps 2-9 read the
+// other accumulator (warp w: rows 32(w%4)..+31, alternate 16-column groups)
+// and append every (query, row) whose score reaches the query's threshold.
+// The query tile is loaded once per CTA.  Waits are bounded as in
+// gemm_ws_kernel and set the same error flag.
+constexpr int SEL_STAGES_MAX = 6, SEL_EPI_WARPS = 8, SEL_THREADS = 32 * (2 + SEL_EPI_WARPS);
+constexpr int SEL_TILE_BYTES = 128 * SK;          // 32 KB: two 16 KB K halves
+
+__device__ __forceinline__ uint32_t sel_idesc(int N) {
+  return (1u << 4)                                // D format F32; A, B format E4M3 (0)
+       | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(SEL_THREADS, 1)
+    score_select_tc_kernel(const __grid_constant__ CUtensorMap map_db,
+                           const __grid_constant__ CUtensorMap map_q, SelArgs a, int N,
+                           int stages, int* err) {
+  extern __shared__ __align__(1024) unsigned char xsm[];
+  const uint32_t raw = smem_u32(xsm);
+  unsigned char* base = xsm + ((1024 - (raw & 1023)) & 1023);
+  unsigned char* sq = base;                                   // [2][N][128]
+  unsigned char* tiles = base + (size_t)N * SK;               // [stages][2][128][128]
+  __shared__ __align__(8) uint64_t full[SEL_STAGES_MAX], empty[SEL_STAGES_MAX];
+  __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], q_full, mma_done;
+  __shared__ float tau_s[256];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ volatile int abort_s;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q0 = blockIdx.y * N;
+  const int64_t ntiles = (a.n + 127) / 128;
+  uint32_t tcols = 32;
+  while (tcols < (uint32_t)(2 * N)) tcols <<= 1;
+
+  for (int i = tid; i < N; i += blockDim.x)
+    tau_s[i] = q0 + i < a.nq ? a.tau[q0 + i] : INFINITY;
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base_s)), "r"(tcols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < stages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&full[s])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&empty[s])), "r"(1));
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&acc_full[b])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                   :: "r"(smem_u32(&acc_empty[b])), "r"(SEL_EPI_WARPS));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&q_full)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mma_done)), "r"(1));
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+  auto fail = [&]() {
+    abort_s = 1;
+    atomicExch(err, 1);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ loader
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" :: "l"(&map_db) : "memory");
+      asm volatile("prefetch.tensormap [%0];" :: "l"(&map_q) : "memory");
+      const uint32_t qb = smem_u32(&q_full);
+      mbar_expect_tx(qb, (uint32_t)(N * SK));
+      tma_load_2d(smem_u32(sq), &map_q, 0, q0, qb);
+      tma_load_2d(smem_u32(sq + N * 128), &map_q, 128, q0, qb);
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t loads[SEL_STAGES_MAX] = {};
+      for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+        if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1)) { fail(); break; }
+        const uint32_t fb = smem_u32(&full[stage]);
+        mbar_expect_tx(fb, (uint32_t)SEL_TILE_BYTES);
+        const uint32_t d = smem_u32(tiles + stage * SEL_TILE_BYTES);
+        tma_load_2d(d, &map_db, 0, (int)(t * 128), fb);
+        tma_load_2d(d + SEL_TILE_BYTES / 2, &map_db, 128, (int)(t * 128), fb);
+        ++loads[stage];
+        if (++stage == stages) { stage = 0; phase ^= 1; }
+      }
+      // every issued load lands before the CTA exits (see gemm_ws_kernel)
+      if (!mbar_wait(qb, 0)) fail();
+      if (abort_s) {
+        for (int s2 = 0; s2 < stages; ++s2)
+          if (loads[s2] > 0) mbar_wait(smem_u32(&full[s2]), (loads[s2] - 1) & 1u);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issue
+    if (lane == 0) {
+      const uint32_t idesc = sel_idesc(N);
+      const uint32_t qa = smem_u32(sq);
+      bool any = false;
+      if (!mbar_wait(smem_u32(&q_full), 0)) fail();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      int stage = 0;
+      uint32_t phase = 0;
+      int b = 0;
+      uint32_t acc_phase = 0;
+      for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+        if (!mbar_wait(smem_u32(&acc_empty[b]), acc_phase ^ 1)) { fail(); break; }
+        if (!mbar_wait(smem_u32(&full[stage]), phase)) { fail(); break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * N);
+        const uint32_t d0 = smem_u32(tiles + stage * SEL_TILE_BYTES);
+#pragma unroll
+        for (int ks = 0; ks < SK / 32; ++ks) {
+          const uint32_t h = (uint32_t)(ks >> 2), ko = (uint32_t)(ks & 3) * 32;
+          const uint64_t da = umma_desc_sw128(d0 + h * (SEL_TILE_BYTES / 2) + ko);
+          const uint64_t db = umma_desc_sw128(qa + h * (uint32_t)(N * 128) + ko);
+          const uint32_t accum = ks > 0 ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n"
+              :: "r"(acc), "l"(da), "l"(db), "r"(idesc), "r"(accum));
+        }
+        any = true;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&empty[stage])) : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&acc_full[b])) : "memory");
+        if (++stage == stages) { stage = 0; phase ^= 1; }
+        if (++b == 2) { b = 0; acc_phase ^= 1; }
+      }
+      if (any) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&mma_done)) : "memory");
+        if (!mbar_wait(smem_u32(&mma_done), 0)) fail();
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int e = warp - 2;
+    const int qr = warp & 3;                      // tensor-memory lanes 32qr .. 32qr + 31
+    const int c_first = (e >> 2) * 16;            // 16-column groups, alternating halves
+    int b = 0;
+    uint32_t acc_phase = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && !abort_s; t += gridDim.x) {
+      if (!mbar_wait(smem_u32(&acc_full[b]), acc_phase)) { if (lane == 0) fail(); break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int64_t row = t * 128 + qr * 32 + lane;
+#pragma unroll 1
+      for (int c0 = c_first; c0 < N; c0 += 32) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(qr * 32) << 16) + (uint32_t)(b * N + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+            "%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < a.n) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float s = __uint_as_float(v[j]);
+            const int c = c0 + j;
+            if (s >= tau_s[c]) {             // padding columns have tau = +inf
+              const int q = q0 + c;
+              const int slot = atomicAdd(a.count + q, 1);
+              if (slot < a.cap) {
+                a.cand[(int64_t)q * a.cap + slot] = row;
+                a.cand_score[(int64_t)q * a.cap + slot] = s;
+              }
+            }
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+      if (++b == 2) { b = 0; acc_phase ^= 1; }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(tcols));
+}
+
 // Residue classes of sequences placed in the padded row layout: row
 // row0[s] + i holds the class (0..19 as ARNDCQEGHILKMFPSTWYV, 20 for any
 // other byte) of byte off[s] + i, i < len[s]; other rows are left as set
@@ -1345,6 +1542,28 @@ static bool make_map(CUtensorMap* map, const void* base, int64_t row_len, int64_
   const cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// Tensor map of `rows` FP8 codes of 256 bytes (row-major, packed), boxes of
+// 128 bytes x box_rows, 128-byte swizzle; rows past the end read as zero.
+static bool make_map_u8(CUtensorMap* map, const void* base, int64_t rows, int box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)SK, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)SK};
+  const cuuint32_t box[2] = {128, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides,
                 box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
@@ -1603,6 +1822,28 @@ extern "C" int sseqs_score_select(const uint8_t* Q, int nq, const uint8_t* DB, i
   if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(DB) & 15))
     return SSEQS_ERR_ARG;
   SelArgs a{Q, nq, DB, n, tau, count, cand, cand_score, cap};
+  if (g_tc_enabled && n < (int64_t)INT32_MAX - 256) {
+    // tcgen05: query tiles of N = the batch rounded up to 16 (at most 256)
+    int* err = tc_err_ptr();
+    if (!err) return SSEQS_ERR_CUDA;
+    const int N = std::min(256, (nq + 15) / 16 * 16);
+    const int qt = (nq + N - 1) / N;
+    const int stages = (int)std::min<int64_t>(
+        SEL_STAGES_MAX, (227 * 1024 - 4096 - (int64_t)N * SK) / SEL_TILE_BYTES);
+    const size_t smem = (size_t)N * SK + (size_t)stages * SEL_TILE_BYTES + 1024;
+    CUtensorMap mdb, mq;
+    if (!make_map_u8(&mdb, DB, n, 128) || !make_map_u8(&mq, Q, nq, N)) return SSEQS_ERR_CUDA;
+    if (cudaFuncSetAttribute((const void*)score_select_tc_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return SSEQS_ERR_CUDA;
+    const int64_t ntiles = (n + 127) / 128;
+    const int per_tile = std::max(1, device_sm_count() / qt);
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, per_tile));
+    { score_select_tc_kernel<<<dim3(gx, qt), SEL_THREADS, smem, stream>>>(mdb, mq, a, N, stages,
+                                                                            err);
+      count_launches(1); }
+    return status_of(cudaGetLastError());
+  }
   const size_t smem = score_smem(2);
   if (cudaFuncSetAttribute((const void*)score_select_kernel,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

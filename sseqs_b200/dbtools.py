@@ -71,15 +71,18 @@ def _geometric(shape, gen, device, p=0.5):
 
 
 def plant_homologs(query: str, n: int, ident_lo: float, ident_hi: float, gen, device,
-                   indel_rate: float = 0.02, cdf=None):
+                   indel_rate: float = 0.02, cdf=None, with_identity: bool = False):
     """``n`` mutated copies of ``query``: per copy an identity u ~ U(lo, hi);
     each residue is replaced by a background residue with probability 1-u;
     at each position a deletion (rate/2) or insertion (rate/2) event of
-    geometric length starts.  Returns (residue bytes, lengths)."""
+    geometric length starts.  Returns (residue bytes, lengths), and with
+    ``with_identity`` also the u of every copy (float32)."""
     q = torch.tensor(list(query.encode()), dtype=torch.uint8, device=device)
     L = q.numel()
     if n == 0:
-        return torch.empty(0, dtype=torch.uint8, device=device), torch.empty(0, dtype=torch.int64, device=device)
+        out = (torch.empty(0, dtype=torch.uint8, device=device),
+               torch.empty(0, dtype=torch.int64, device=device))
+        return out + (torch.empty(0, dtype=torch.float32, device=device),) if with_identity else out
     ident = ident_lo + (ident_hi - ident_lo) * torch.rand(n, 1, generator=gen, device=device)
     sub = torch.rand(n, L, generator=gen, device=device) >= ident
     sub_res = random_residues(n * L, gen, device, cdf).view(n, L)
@@ -110,6 +113,8 @@ def plant_homologs(query: str, n: int, ident_lo: float, ident_hi: float, gen, de
     is_base = rank < keep.flatten()[src]
     ins_res = random_residues(total, gen, device, cdf)
     res = torch.where(is_base, base.flatten()[src], ins_res)
+    if with_identity:
+        return res, lengths, ident.flatten().to(torch.float32)
     return res, lengths
 
 
@@ -119,6 +124,7 @@ class SyntheticDB:
     n_seqs: int
     n_residues: int
     planted: dict = field(default_factory=dict)   # query index -> db sequence ids
+    planted_identity: dict = field(default_factory=dict)   # query index -> identity u of each
     seq_chunk: torch.Tensor | None = None          # chunk of every sequence
     seq_rank: torch.Tensor | None = None           # position inside its chunk
 
@@ -179,11 +185,14 @@ def synthetic_db(queries: list[str], n_seqs: int, homolog_frac: float, ident: tu
     owner = owner[torch.randperm(n_seqs, generator=gen, device=device)]
     lengths = lognormal_lengths(n_seqs, gen, device)
     homologs = []
+    identity = {}
     for qi, q in enumerate(queries):
-        hb, hl = plant_homologs(q, n_h, ident[0], ident[1], gen, device, cdf=cdf)
+        hb, hl, hu = plant_homologs(q, n_h, ident[0], ident[1], gen, device, cdf=cdf,
+                                    with_identity=True)
         slots = torch.nonzero(owner == qi).flatten()
         lengths[slots] = hl
         homologs.append((slots, hb, hl))
+        identity[qi] = hu
     sizes = lengths + 1
     ends = torch.cumsum(sizes, 0)
     total = int(ends[-1].item())
@@ -202,7 +211,7 @@ def synthetic_db(queries: list[str], n_seqs: int, homolog_frac: float, ident: tu
     n_res = int(lengths.sum().item())
     chunks, seq_chunk, seq_rank = assemble_stream(stream, lengths, chunk_bytes)
     planted = {qi: torch.nonzero(owner == qi).flatten() for qi in range(len(queries))}
-    return SyntheticDB(chunks, n_seqs, n_res, planted, seq_chunk, seq_rank)
+    return SyntheticDB(chunks, n_seqs, n_res, planted, identity, seq_chunk, seq_rank)
 
 
 def pack_symbols_host(sym: np.ndarray) -> np.ndarray:

@@ -25,6 +25,7 @@ for the same stage (it has no reference counterpart):
 """
 from __future__ import annotations
 
+import ctypes
 import importlib
 import math
 from dataclasses import dataclass
@@ -511,10 +512,11 @@ class LearnedIndex:
                                         stream_ptr()), "quantize")
         return codes
 
-    def candidates(self, qcodes: torch.Tensor, n_cand: int, sample: int = 8192,
-                   factor: float = 2.5, cap_factor: int = 8):
-        """Per query the database rows of its ``n_cand`` highest code scores
-        (fewer when fewer pass the threshold); list of int64 tensors."""
+    def _select(self, qcodes: torch.Tensor, n_cand: int, sample: int, factor: float,
+                cap_factor: int):
+        """Threshold per query from a sample of the codes, then every row at
+        or above it by the FP8 selection GEMM: (cand [nq, cap], scores,
+        host counts, cap)."""
         dev = self.db.device
         nq = qcodes.shape[0]
         L = lib()
@@ -540,101 +542,187 @@ class LearnedIndex:
                                        ptr(count), ptr(cand), ptr(cs), cap, stream_ptr()),
                   "score_select")
             cnt = to_host(count)
+            flag = ctypes.c_int(0)
+            check(L.sseqs_gemm_error(ctypes.byref(flag)), "gemm_error")
+            if flag.value:
+                raise RuntimeError("score_select: a bounded wait of the selection kernel ran out")
             if int(cnt.max(initial=0)) <= cap or cap >= self.n:
                 break
             cap = int(min(self.n, 2 * int(cnt.max())))
-        out = []
-        for q in range(nq):
-            c = int(min(cnt[q], cap))
-            if c <= n_cand:
-                out.append(cand[q, :c])
-                continue
-            # lists are appended in no fixed order: order them by row first,
-            # so that ties at the cut go to the lower rows, as in every run
-            rows_q, perm = cand[q, :c].sort()
-            keys = cs[q, :c][perm].to(torch.float16)
-            p = select.topk_indices(keys, n_cand).long()
-            out.append(rows_q[p])
-        return out, cnt
+        return cand, cs, cnt, cap
 
-    def rescore(self, queries, cands, top: int = 4096, gap_open=11, gap_extend=1):
+    def candidates_flat(self, qcodes: torch.Tensor, n_cand: int, sample: int = 8192,
+                        factor: float = 2.5, cap_factor: int = 8):
+        """Per query the database rows of its ``n_cand`` highest code scores
+        (fewer when fewer pass the threshold; ties at the cut go to the lower
+        rows), as device arrays sorted by (query, row): ``(qid, rows)``
+        (int64), and the host count per query."""
+        dev = self.db.device
+        nq = qcodes.shape[0]
+        cand, cs, cnt, cap = self._select(qcodes, n_cand, sample, factor, cap_factor)
+        took = np.minimum(cnt, cap).astype(np.int64)
+        tk = torch.from_numpy(took).to(dev)
+        live = torch.arange(cap, device=dev)[None, :] < tk[:, None]
+        rows = cand[live]                                   # query-major
+        keys = cs[live].to(torch.float16)
+        qid = torch.repeat_interleave(torch.arange(nq, device=dev), tk)
+        # the lists are appended in no fixed order: order by (query, row),
+        # then stably by key (desc) and query, so that inside a query the
+        # keys fall and equal keys keep the lower rows first
+        o = torch.argsort(qid * max(self.n, 1) + rows)
+        o = o[torch.sort(keys[o], descending=True, stable=True).indices]
+        o = o[torch.sort(qid[o], stable=True).indices]
+        start = torch.cumsum(tk, 0) - tk
+        rank = torch.arange(o.numel(), device=dev) - start[qid[o]]
+        o = o[rank < n_cand]
+        kq, kr = qid[o], rows[o]
+        o = torch.argsort(kq * max(self.n, 1) + kr)
+        return kq[o], kr[o], np.minimum(took, n_cand)
+
+    def candidates(self, qcodes: torch.Tensor, n_cand: int, sample: int = 8192,
+                   factor: float = 2.5, cap_factor: int = 8):
+        """``candidates_flat`` as a list of row tensors (increasing), one per
+        query, and the host counts of rows at or above each threshold."""
+        kq, kr, counts = self.candidates_flat(qcodes, n_cand, sample, factor, cap_factor)
+        return list(torch.split(kr, [int(c) for c in counts])), counts
+
+    def _batch_tables(self):
+        if getattr(self, "_tabs", None) is None:
+            dev = self.db.device
+            bs = self.db.batches
+            seg = [b.seg_index[:b.n_segments].to(torch.int32) for b in bs]
+            self._tabs = {
+                "cum": torch.from_numpy(self.cum).to(dev),
+                "nseg": torch.tensor([b.n_segments for b in bs] or [0], dtype=torch.int64,
+                                     device=dev),
+                "maxlen": torch.tensor([b.maxlen for b in bs] or [0], dtype=torch.int64,
+                                       device=dev),
+                # segment number of every index row (the delimiter-based index
+                # the exhaustive search reports)
+                "seg": torch.cat(seg) if seg else torch.zeros(1, dtype=torch.int32, device=dev),
+            }
+        return self._tabs
+
+    def rescore_flat(self, queries, qid: torch.Tensor, rows: torch.Tensor, top: int = 4096,
+                     gap_open=11, gap_extend=1) -> list:
         """Exact affine SW of every query against its candidate rows (the
         affine stage of sseqs/msa.py:327-337: skip 1 residue, first and last
-        segment of a batch excluded); returns per query the ``top`` hits as
-        rows (normalised score, batch, segment, affine score) -- segment being
-        the delimiter-based index the exhaustive search reports -- sorted by
-        normalised score desc, then batch, then segment."""
+        segment of a batch excluded).  ``qid``/``rows``: device int64, sorted
+        by (query, row).  Returns per query the ``top`` hits as host arrays
+        ``(norm float32, batch, segment, affine int64)`` sorted by normalised
+        score desc, then batch, then segment.
+
+        The work per engine step does not grow with the number of database
+        batches beyond one SW launch per (batch, stripe-width group): the
+        target lists, their positions and the ranking are built with a fixed
+        number of whole-array operations, and the hits come back in one copy
+        per field."""
         from . import batched
         sw = importlib.import_module("sseqs_b200.sw")
         dev = self.db.device
+        nq, nb = len(queries), len(self.db.batches)
+        empty = (np.zeros(0, np.float32), np.zeros(0, np.int64), np.zeros(0, np.int64),
+                 np.zeros(0, np.int64))
+        if nq == 0 or rows.numel() == 0 or nb == 0:
+            return [empty for _ in range(nq)]
+        T = self._batch_tables()
         enc = [sw.encode_query(q, device=dev) for q in queries]
-        nb = len(self.db.batches)
-        # per query its candidate rows in order, and where each batch's
-        # scored segments (1 .. n-2) begin and end among them: one small
-        # device-to-host copy per query
-        bounds = torch.tensor([[int(self.cum[bi]) + 1, int(self.cum[bi]) + b.n_segments - 1]
-                               for bi, b in enumerate(self.db.batches)],
-                              dtype=torch.int64, device=dev).reshape(-1)
-        rows_sorted, cuts = [], []
-        for c in cands:
-            r = c.sort().values
-            rows_sorted.append(r)
-            cuts.append(torch.searchsorted(r, bounds))
-        cuts = to_host(torch.stack(cuts)).reshape(len(cands), nb, 2) if cands else None
-        parts = [[] for _ in queries]          # (batch, segment ids, scores) on the device
-        for bi, b in enumerate(self.db.batches):
-            lists = [rows_sorted[qi][int(cuts[qi, bi, 0]):int(cuts[qi, bi, 1])] -
-                     int(self.cum[bi]) for qi in range(len(queries))]
-            for tpt, members in batched.buckets([e.numel() for e in enc]).items():
-                for s0 in range(0, len(members), batched.GROUP):
-                    grp = [qi for qi in members[s0:s0 + batched.GROUP] if lists[qi].numel()]
-                    if not grp:
-                        continue
-                    m = max(lists[qi].numel() for qi in grp)
-                    idx = torch.empty((len(grp), m), dtype=torch.int32, device=dev)
-                    segs = []
-                    for j, qi in enumerate(grp):
-                        g = b.seg_index[lists[qi]].to(torch.int32)
-                        idx[j, :g.numel()] = g
-                        idx[j, g.numel():] = g[-1]
-                        segs.append(g)
-                    qbuf = torch.zeros((len(grp), batched.MAX_QUERY), dtype=torch.uint8,
-                                       device=dev)
-                    for j, qi in enumerate(grp):
-                        qbuf[j, :enc[qi].numel()] = enc[qi]
-                    ql = torch.tensor([enc[qi].numel() for qi in grp], dtype=torch.int32,
-                                      device=dev)
-                    sc = batched.sw_scan_queries(qbuf, ql, tpt, b.ascii, b.delim, affine=True,
-                                                 good_idx=idx, skip=1, gap_a=gap_open,
-                                                 gap_b=gap_extend)
-                    for j, qi in enumerate(grp):
-                        parts[qi].append((bi, segs[j], sc[j, :segs[j].numel()]))
-        # rank per query: normalised score desc, then batch, then segment
-        out = []
-        for qi, q in enumerate(queries):
-            if not parts[qi]:
-                out.append([])
-                continue
-            Lq = len(q)
-            seg = to_host(torch.cat([p[1] for p in parts[qi]])).astype(np.int64)
-            aff = to_host(torch.cat([p[2] for p in parts[qi]]))
-            bat = np.concatenate([np.full(p[1].numel(), p[0], np.int64) for p in parts[qi]])
-            mx = np.concatenate([np.full(p[1].numel(), self.db.batches[p[0]].maxlen, np.int64)
-                                 for p in parts[qi]])
-            norm = np.empty(aff.size, np.float32)
-            for ml in np.unique(mx):
-                sel = mx == ml
-                norm[sel] = (aff[sel].astype(np.float32) /
-                             np.sqrt(np.float32(Lq * int(ml)))).astype(np.float32)
-            keep = np.lexsort((seg, bat, -norm.astype(np.float64)))[:top]
-            out.append(list(zip(norm[keep].tolist(), bat[keep].tolist(), seg[keep].tolist(),
-                                aff[keep].astype(np.int64).tolist())))
-        return out
+        lens = [e.numel() for e in enc]
+        batch = torch.searchsorted(T["cum"][1:], rows, right=True)
+        local = rows - T["cum"][batch]
+        ok = (local >= 1) & (local <= T["nseg"][batch] - 2)
+        qid, rows, batch = qid[ok], rows[ok], batch[ok]
+        seg = T["seg"][rows]
+        n = qid.numel()
+        if n == 0:
+            return [empty for _ in range(nq)]
+        # candidates per (query, batch): contiguous runs of the flat order
+        cqb = to_host(torch.bincount(qid * nb + batch, minlength=nq * nb)).reshape(nq, nb)
+        cqb = cqb.astype(np.int64)
+        start = (np.cumsum(cqb.reshape(-1)) - cqb.reshape(-1)).reshape(nq, nb)
+        # launches: per batch, per stripe width, up to GROUP queries; every
+        # query row of a launch holds its own targets, padded with its last
+        plan, pos_parts, qid_parts = [], [], []
+        pos_off = q_off = 0
+        bk = batched.buckets(lens)
+        for bi in range(nb):
+            for tpt, members in bk.items():
+                live_q = [q for q in members if cqb[q, bi] > 0]
+                for s0 in range(0, len(live_q), batched.GROUP):
+                    grp = live_q[s0:s0 + batched.GROUP]
+                    cnt = cqb[grp, bi]
+                    m = int(cnt.max())
+                    k = np.minimum(np.arange(m)[None, :], cnt[:, None] - 1)
+                    pos_parts.append((start[grp, bi][:, None] + k).reshape(-1))
+                    qid_parts.append(np.asarray(grp, np.int64))
+                    plan.append((bi, tpt, len(grp), m, pos_off, q_off))
+                    pos_off += len(grp) * m
+                    q_off += len(grp)
+        pos = torch.from_numpy(np.concatenate(pos_parts)).to(dev)
+        lq = torch.from_numpy(np.concatenate(qid_parts)).to(dev)
+        idx_all = seg[pos]
+        qbuf = torch.zeros((nq, batched.MAX_QUERY), dtype=torch.uint8, device=dev)
+        for j, e in enumerate(enc):
+            qbuf[j, :e.numel()] = e
+        qlen = torch.tensor(lens, dtype=torch.int32, device=dev)
+        qrows, qls = qbuf[lq], qlen[lq]
+        aff = torch.empty(n, dtype=torch.int32, device=dev)
+        for bi, tpt, G, m, po, qo in plan:
+            b = self.db.batches[bi]
+            sc = batched.sw_scan_queries(qrows[qo:qo + G], qls[qo:qo + G], tpt, b.ascii,
+                                         b.delim, affine=True,
+                                         good_idx=idx_all[po:po + G * m].view(G, m), skip=1,
+                                         gap_a=gap_open, gap_b=gap_extend)
+            aff.index_copy_(0, pos[po:po + G * m], sc[:, :m].reshape(-1))
+        # normalised score as the exhaustive search forms it (float32 of the
+        # affine score over float32 sqrt of Lq * maxlen of the hit's batch)
+        den = torch.sqrt((qlen.to(torch.int64)[qid] * T["maxlen"][batch]).to(torch.float32))
+        norm = aff.to(torch.float32) / den
+        # rank: inside each query normalised score desc; the flat order is
+        # (batch, segment) ascending, which the stable sorts keep for ties
+        o = torch.sort(norm, descending=True, stable=True).indices
+        o = o[torch.sort(qid[o], stable=True).indices]
+        per_q = cqb.sum(1)
+        qstart = torch.from_numpy(np.cumsum(per_q) - per_q).to(dev)
+        rank = torch.arange(n, device=dev) - qstart[qid[o]]
+        o = o[rank < top]
+        keep = np.minimum(per_q, top)
+        h_norm, h_b = to_host(norm[o]), to_host(batch[o])
+        h_s, h_a = to_host(seg[o]), to_host(aff[o])
+        cuts = np.cumsum(keep)[:-1]
+        return [(a_, b_.astype(np.int64), c_.astype(np.int64), d_.astype(np.int64))
+                for a_, b_, c_, d_ in zip(np.split(h_norm, cuts), np.split(h_b, cuts),
+                                          np.split(h_s, cuts), np.split(h_a, cuts))]
+
+    def rescore(self, queries, cands, top: int = 4096, gap_open=11, gap_extend=1):
+        """``rescore_flat`` of per-query candidate row tensors; returns per
+        query the ``top`` hits as rows (normalised score, batch, segment,
+        affine score) sorted by normalised score desc, then batch, then
+        segment."""
+        dev = self.db.device
+        counts = [int(c.numel()) for c in cands]
+        if sum(counts) == 0:
+            return [[] for _ in queries]
+        rows = torch.cat([c.to(dev, torch.int64) for c in cands])
+        qid = torch.repeat_interleave(torch.arange(len(cands), device=dev),
+                                      torch.tensor(counts, device=dev))
+        o = torch.argsort(qid * max(self.n, 1) + rows)
+        res = self.rescore_flat(queries, qid[o], rows[o], top, gap_open, gap_extend)
+        return [list(zip(r[0].tolist(), r[1].tolist(), r[2].tolist(), r[3].tolist()))
+                for r in res]
+
+    def search_arrays(self, queries, n_cand: int = 32768, top: int = 4096, **kw) -> list:
+        """``rescore_flat`` of the candidates of ``queries``: per query host
+        arrays (norm, batch, segment, affine)."""
+        codes = self.query_codes(queries)
+        kq, kr, _ = self.candidates_flat(codes, n_cand, **kw)
+        return self.rescore_flat(queries, kq, kr, top=top)
 
     def search(self, queries, n_cand: int = 32768, top: int = 4096, **kw):
-        codes = self.query_codes(queries)
-        cands, _ = self.candidates(codes, n_cand, **kw)
-        return self.rescore(queries, cands, top=top)
+        """Per query the ``top`` hits as rows (normalised score, batch,
+        segment, affine score)."""
+        return [list(zip(r[0].tolist(), r[1].tolist(), r[2].tolist(), r[3].tolist()))
+                for r in self.search_arrays(queries, n_cand, top, **kw)]
 
 
 def hit_strings(db, rows, width: int = 500) -> list:

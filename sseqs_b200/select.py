@@ -18,8 +18,10 @@ def find_delims(ascii: torch.Tensor, count: torch.Tensor | None = None,
                 max_out: int | None = None, sync: bool = True):
     """Positions (int32) of every '@' byte of ``ascii``.
 
-    With ``sync`` the result is trimmed to the count (one host read);
-    otherwise ``(positions[max_out], count_dev)`` is returned.
+    With ``sync`` the result is copied out at its exact size (one host
+    read), so a resident table does not pin the ``max_out``-sized scratch
+    (four bytes per input byte); otherwise ``(positions[max_out],
+    count_dev)`` is returned.
     """
     n = ascii.numel()
     L = lib()
@@ -32,7 +34,8 @@ def find_delims(ascii: torch.Tensor, count: torch.Tensor | None = None,
                               stream_ptr()), "find_delims")
     if not sync:
         return out, cnt
-    return out[: int(cnt.item())]
+    c = int(cnt.item())
+    return out[:c].clone() if c < out.numel() else out
 
 
 def segment_table(ascii: torch.Tensor, delim: torch.Tensor) -> dict:

@@ -167,19 +167,11 @@ class LearnedExecutor:
         req.enc = req.query
 
     def step(self, bi: int, reqs: list) -> list:
-        queries = [r.enc for r in reqs]
-        codes = self.index.query_codes(queries)
-        cands, _ = self.index.candidates(codes, self.n_cand)
-        rows = self.index.rescore(queries, cands, top=self.top_k)
-        out = []
-        for rr in rows:
-            # (segment, score) with the batch folded into the order; the
-            # server's merge sorts by score, then batch, then segment
-            seg = np.array([r[2] for r in rr], dtype=np.int32)
-            sc = np.array([r[3] for r in rr], dtype=np.int32)
-            bt = np.array([r[1] for r in rr], dtype=np.int32)
-            out.append((seg, sc, bt))
-        return out
+        res = self.index.search_arrays([r.enc for r in reqs], n_cand=self.n_cand, top=self.top_k)
+        # (segment, score, batch) per request; the server's merge sorts by
+        # score, then batch, then segment
+        return [(seg.astype(np.int32), aff.astype(np.int32), bt.astype(np.int32))
+                for _, bt, seg, aff in res]
 
 
 class SearchServer:

@@ -235,11 +235,10 @@ def test_embedder_backward_matches_autograd(residual):
     assert close(grads["emb"], Ep.grad) > 0.99
 
 
-def test_score_select_and_threshold():
-    from sseqs_b200 import _lib, learned
+def _codes(nq, n, seed=1):
+    from sseqs_b200 import _lib
     g = torch.Generator(device="cpu")
-    g.manual_seed(1)
-    nq, n = 130, 5000
+    g.manual_seed(seed)
     q = torch.randn(nq, 256, generator=g)
     d = torch.randn(n, 256, generator=g)
     q = (q / q.norm(dim=1, keepdim=True)).cuda()
@@ -249,31 +248,76 @@ def test_score_select_and_threshold():
     dc = torch.empty((n, 256), dtype=torch.uint8, device="cuda")
     _lib.check(L.sseqs_quantize_e4m3(q.data_ptr(), q.numel(), 16.0, qc.data_ptr(), 0), "q")
     _lib.check(L.sseqs_quantize_e4m3(d.data_ptr(), d.numel(), 16.0, dc.data_ptr(), 0), "q")
+    return qc, dc
+
+
+def _select(qc, dc, tau, cap):
+    from sseqs_b200 import _lib
+    nq, n = qc.shape[0], dc.shape[0]
+    cnt = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    cand = torch.empty((nq, cap), dtype=torch.int64, device="cuda")
+    cs = torch.empty((nq, cap), dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib().sseqs_score_select(qc.data_ptr(), nq, dc.data_ptr(), n, tau.data_ptr(),
+                                             cnt.data_ptr(), cand.data_ptr(), cs.data_ptr(), cap,
+                                             0), "select")
+    return cnt, cand, cs
+
+
+def test_score_select_and_threshold():
+    from sseqs_b200 import _lib
+    nq, n = 130, 5000
+    qc, dc = _codes(nq, n)
+    L = _lib.lib()
     qf = qc.view(torch.float8_e4m3fn).float()
     df = dc.view(torch.float8_e4m3fn).float()
     ref = qf @ df.T                                             # fp32 reference
     dense = torch.empty((nq, n), dtype=torch.float32, device="cuda")
     _lib.check(L.sseqs_score_dense(qc.data_ptr(), nq, dc.data_ptr(), n, dense.data_ptr(), 0), "d")
     assert (dense - ref).abs().max().item() < 1e-3
-    tau = torch.quantile(ref, 0.99, dim=1).contiguous()
-    cap = 200
-    cnt = torch.zeros(nq, dtype=torch.int32, device="cuda")
-    cand = torch.empty((nq, cap), dtype=torch.int64, device="cuda")
-    cs = torch.empty((nq, cap), dtype=torch.float32, device="cuda")
-    _lib.check(L.sseqs_score_select(qc.data_ptr(), nq, dc.data_ptr(), n, tau.data_ptr(),
-                                    cnt.data_ptr(), cand.data_ptr(), cs.data_ptr(), cap, 0), "s")
-    for i in range(nq):
-        c = int(cnt[i])
-        assert c <= cap
-        got = set(cand[i, :c].tolist())
-        sure_in = set(torch.nonzero(ref[i] >= tau[i] + 1e-3).flatten().tolist())
-        maybe = set(torch.nonzero(ref[i] >= tau[i] - 1e-3).flatten().tolist())
-        assert sure_in <= got <= maybe
     k = 7
     kth = torch.empty(nq, dtype=torch.float32, device="cuda")
     sub = ref[:, :4000].contiguous()
     _lib.check(L.sseqs_kth_largest_rows(sub.data_ptr(), nq, 4000, k, kth.data_ptr(), 0), "k")
     assert torch.equal(kth, torch.topk(sub, k, dim=1).values[:, -1])
+
+
+# batch sizes: one query, a partial 16-column tile, exactly 256 (one full
+# tcgen05 query tile), 300 (two tiles, the second ragged); database sizes
+# with and without a partial 128-row tile
+@pytest.mark.parametrize("nq,n", [(1, 5000), (8, 4096), (37, 5000), (130, 5000),
+                                  (256, 3000), (300, 2000)])
+@pytest.mark.parametrize("path", [1, 0])    # 1: tcgen05 kind::f8f6f4, 0: mma.sync
+def test_score_select_paths(nq, n, path):
+    """Every (query, row) at least 1e-3 above the query's threshold is
+    selected and none more than 1e-3 below it (fp32 reference of the FP8
+    dot products); the scores reported are the reference's within 1e-3;
+    both paths select the same sets apart from rows within 1e-3 of a
+    threshold."""
+    from sseqs_b200 import _lib
+    qc, dc = _codes(nq, n, seed=nq + n)
+    qf = qc.view(torch.float8_e4m3fn).float()
+    df = dc.view(torch.float8_e4m3fn).float()
+    ref = qf @ df.T
+    tau = torch.quantile(ref, 0.99, dim=1).contiguous()
+    cap = 200
+    _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(path), "path")
+    try:
+        cnt, cand, cs = _select(qc, dc, tau, cap)
+        torch.cuda.synchronize()
+    finally:
+        _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(1), "path")
+    assert _gemm_error() == 0
+    for i in range(nq):
+        c = int(cnt[i])
+        assert c <= cap
+        rows = cand[i, :c]
+        got = set(rows.tolist())
+        assert len(got) == c
+        sure_in = set(torch.nonzero(ref[i] >= tau[i] + 1e-3).flatten().tolist())
+        maybe = set(torch.nonzero(ref[i] >= tau[i] - 1e-3).flatten().tolist())
+        assert sure_in <= got <= maybe
+        if c:
+            assert (cs[i, :c] - ref[i, rows]).abs().max().item() < 1e-3
 
 
 def test_learned_search_reports_exact_scores():
@@ -299,3 +343,86 @@ def test_learned_search_reports_exact_scores():
                          skip=1, gap_a=11, gap_b=1)
         assert int(exp[0]) == score
         assert abs(norm - score / math.sqrt(len(q0) * b.maxlen)) < 1e-5
+
+
+def _ragged_db(n_seqs=3000, chunk_bytes=100_000, seed=3):
+    """Several batches with empty segments ('@@') among the sequences."""
+    from sseqs_b200 import dbtools
+    from sseqs_b200.database import Database
+    rng = np.random.default_rng(seed)
+    seqs = ["" if rng.random() < 0.03 else dbtools.random_query(int(rng.integers(20, 400)),
+                                                                90000 + i)
+            for i in range(n_seqs)]
+    raw = b"".join(s.encode() + b"@" for s in seqs)
+    stream = torch.from_numpy(np.frombuffer(raw, np.uint8).copy())
+    lengths = torch.tensor([len(s) for s in seqs], dtype=torch.int64)
+    chunks, _, _ = dbtools.assemble_stream(stream, lengths, chunk_bytes)
+    return Database(chunks, bs=chunk_bytes)
+
+
+def test_rescore_matches_direct_scoring():
+    """Rescoring of explicit candidate lists (random rows plus the first and
+    last row of every batch, which are not scored) on a multi-batch database
+    with empty segments, queries of several stripe widths: the same hits, in
+    the same order, as scoring every candidate directly and ranking by
+    normalised score desc, then batch, then segment."""
+    from sseqs_b200 import dbtools, learned
+    sw = importlib.import_module("sseqs_b200.sw")
+    db = _ragged_db()
+    assert len(db.batches) >= 4
+    idx = learned.LearnedIndex(learned.Embedder(seed=4), db, chunk=1000)
+    rng = np.random.default_rng(5)
+    queries = [dbtools.random_query(L, 500 + j)
+               for j, L in enumerate([40, 150, 151, 300, 700, 33, 1000])]
+    edges = np.concatenate([idx.cum[:-1], idx.cum[1:] - 1])
+    cands = [torch.from_numpy(np.unique(np.concatenate(
+        [rng.choice(idx.n, size=min(idx.n, 400), replace=False), edges]))).cuda()
+        for _ in queries]
+    top = 150
+    got = idx.rescore(queries, cands, top=top)
+    for j, q in enumerate(queries):
+        enc = sw.encode_query(q)
+        rows = cands[j].cpu().numpy()
+        bat = np.searchsorted(idx.cum[1:], rows, side="right")
+        loc = rows - idx.cum[bat]
+        S, B, G, A = [], [], [], []
+        for bi in np.unique(bat):
+            b = db.batches[bi]
+            sel = (bat == bi) & (loc >= 1) & (loc <= b.n_segments - 2)
+            if not sel.any():
+                continue
+            g = b.seg_index[torch.from_numpy(loc[sel]).cuda()].to(torch.int32)
+            sc = sw.sw_scan(enc, b.ascii, b.delim, affine=True, good_idx=g, skip=1, gap_a=11,
+                            gap_b=1).cpu().numpy().astype(np.int64)
+            A.append(sc)
+            G.append(g.cpu().numpy().astype(np.int64))
+            B.append(np.full(sc.size, bi, np.int64))
+            S.append((sc.astype(np.float32) / np.sqrt(np.float32(len(q) * b.maxlen)))
+                     .astype(np.float32))
+        S, B, G, A = (np.concatenate(x) for x in (S, B, G, A))
+        o = np.lexsort((G, B, -S.astype(np.float64)))[:top]
+        want = list(zip(S[o].tolist(), B[o].tolist(), G[o].tolist(), A[o].tolist()))
+        assert got[j] == want
+
+
+def test_candidates_take_top_keys_with_lower_rows_at_ties():
+    """The per-query cut of the selection: the n_cand largest fp16 keys,
+    ties at the cut to the lower rows (against the raw selection lists)."""
+    from sseqs_b200 import dbtools, learned
+    db = _ragged_db(seed=6)
+    idx = learned.LearnedIndex(learned.Embedder(seed=6), db, chunk=1000)
+    queries = [dbtools.random_query(L, 700 + j) for j, L in enumerate([60, 250, 512])]
+    codes = idx.query_codes(queries)
+    n_cand = 50
+    cand, cs, cnt, cap = idx._select(codes, n_cand, 8192, 2.5, 8)
+    kq, kr, counts = idx.candidates_flat(codes, n_cand)
+    kq, kr = kq.cpu().numpy(), kr.cpu().numpy()
+    for j in range(len(queries)):
+        c = int(min(cnt[j], cap))
+        assert c > n_cand                  # the cut is exercised
+        rows = cand[j, :c].cpu().numpy()
+        keys = cs[j, :c].to(torch.float16).float().cpu().numpy()
+        want = np.sort(rows[np.lexsort((rows, -keys.astype(np.float64)))[:n_cand]])
+        mine = kr[kq == j]
+        assert counts[j] == n_cand
+        assert np.array_equal(mine, want)
