@@ -528,6 +528,166 @@ def serving_sweep(index, rates, seconds, seed=6, n_alone=4):
             "index_rows": index.n, "lengths": "U(50, 1000)"}
 
 
+RECALL_BANDS = ((0.20, 0.30), (0.30, 0.45), (0.45, 0.60), (0.60, 0.95))
+
+
+def bench_learned_scale(args):
+    """``--learned-scale``: the learned prefilter at its stated size.  The
+    embedder is trained on ``--learned-pairs`` seeded pairs; the database is
+    20M synthetic sequences in which each of ``--recall-queries`` queries has
+    ``--recall-homologs`` planted homologs (identity U(20%, 95%), the
+    benchmark's length and composition model); ``--learned-queries`` queries
+    are timed (the recall queries first, then U(50, 1000) queries without
+    homologs).  The exact reference is the exhaustive affine sweep of every
+    segment (``batched.BatchedSearcher``, ranked by normalised score like the
+    learned path), timed on the recall queries.  Recall of the exact top-1000
+    over the recall queries, overall and per identity band of the planted
+    homologs among those 1000.  Neither path aligns its hits here.  One JSON
+    line."""
+    import torch
+    from sseqs_b200 import batched, dbtools, learned
+    from sseqs_b200.database import Database
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    rng = np.random.default_rng(41)
+    nr = int(args.recall_queries)
+    recall_qs = [dbtools.random_query(int(L), 40000 + i)
+                 for i, L in enumerate(rng.integers(50, 1001, nr))]
+    n_seqs = int(args.db_seqs)
+    syn = dbtools.synthetic_db(recall_qs, n_seqs, args.recall_homologs / n_seqs, IDENT,
+                               seed=77, device="cuda")
+    db = Database(syn.chunks, bs=BS)
+    batch_of_chunk = {b.chunk: bi for bi, b in enumerate(db.batches) if b.index == 0}
+    seq_chunk, seq_rank = syn.seq_chunk.cpu().numpy(), syn.seq_rank.cpu().numpy()
+    planted = {}                         # query -> {(batch, segment): identity}
+    for qi in range(nr):
+        sid = syn.planted[qi].cpu().numpy()
+        u = syn.planted_identity[qi].cpu().numpy()
+        planted[qi] = {(batch_of_chunk[int(seq_chunk[s])], int(seq_rank[s])): float(x)
+                       for s, x in zip(sid, u)}
+    n_res = syn.n_residues
+    del syn
+    torch.cuda.empty_cache()
+    t1 = time.time()
+    pairs = learned.training_pairs(max(1, args.learned_pairs // 256), 256, seed=5)
+    t2 = time.time()
+    model = learned.Embedder(seed=5)
+    hist = learned.train(model, pairs, epochs=args.learned_epochs, seed=5)
+    n_pairs = int(pairs.y.numel())
+    del pairs
+    torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    t3 = time.time()
+    index = learned.LearnedIndex(model, db)
+    torch.cuda.synchronize()
+    t4 = time.time()
+    qs = recall_qs + [dbtools.random_query(int(L), 60000 + i) for i, L in
+                      enumerate(rng.integers(50, 1001, max(0, args.learned_queries - nr)))]
+    chunk = 256
+    index.search_arrays(qs[:4], n_cand=32768, top=TOP_K)            # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    got = []
+    for s0 in range(0, len(qs), chunk):
+        got += index.search_arrays(qs[s0:s0 + chunk], n_cand=32768, top=TOP_K)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_learned = e0.elapsed_time(e1)
+    e0.record()
+    got_r = []
+    for s0 in range(0, nr, chunk):
+        got_r += index.search_arrays(recall_qs[s0:s0 + chunk], n_cand=32768, top=TOP_K)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_learned_r = e0.elapsed_time(e1)
+    # exhaustive sweep (eager launches; the autotuner runs on two queries first)
+    exact = batched.BatchedSearcher(db, top_k=TOP_K, use_graphs=False)
+    exact.search(recall_qs[:2], rank="norm")
+    torch.cuda.synchronize()
+    e0.record()
+    ref = exact.search(recall_qs, rank="norm")
+    e1.record()
+    torch.cuda.synchronize()
+    ms_exact = e0.elapsed_time(e1)
+    def recall(hits, depth_label):
+        rec, same = [], True
+        band_want = np.zeros(len(RECALL_BANDS), np.int64)
+        band_got = np.zeros(len(RECALL_BANDS), np.int64)
+        band_planted = np.zeros(len(RECALL_BANDS), np.int64)
+        hom_want = hom_got = 0
+        for qi in range(nr):
+            h = ref[qi]
+            want = set(zip(h.batch[:1000].tolist(), h.segment[:1000].tolist()))
+            mine = hits[qi]
+            gset = set(zip(mine[1][:1000].tolist(), mine[2][:1000].tolist()))
+            rec.append(len(want & gset) / max(1, len(want)))
+            # every learned hit's score is the exact score of the same segment
+            ex = dict(zip(zip(h.batch.tolist(), h.segment.tolist()), h.scores.tolist()))
+            for bt, sg, a in zip(mine[1].tolist(), mine[2].tolist(), mine[3].tolist()):
+                if (bt, sg) in ex and ex[(bt, sg)] != a:
+                    same = False
+            for key, u in planted[qi].items():
+                for k, (lo, hi) in enumerate(RECALL_BANDS):
+                    if lo <= u < hi or (k == len(RECALL_BANDS) - 1 and u == hi):
+                        band_planted[k] += 1
+                        if key in want:
+                            band_want[k] += 1
+                            band_got[k] += key in gset
+                            hom_want += 1
+                            hom_got += key in gset
+        bands = [{"identity": [lo, hi], "planted": int(p), "in_exact_top1000": int(w),
+                  "recall": round(float(g) / w, 4) if w else None}
+                 for (lo, hi), p, w, g in zip(RECALL_BANDS, band_planted, band_want, band_got)]
+        return {"candidates_per_query": depth_label,
+                "recall_of_exact_top1000": round(float(np.mean(rec)), 4),
+                "recall_min": round(float(np.min(rec)), 4),
+                "recall_of_planted_homologs_in_exact_top1000":
+                    round(hom_got / max(1, hom_want), 4),
+                "recall_by_identity_band": bands, "scores_equal_exact": same}
+
+    r32 = recall(got_r, 32768)
+    depths = [dict(r32, queries_per_s=round(nr / (ms_learned_r * 1e-3), 2))]
+    for depth in (131072, 524288):
+        e0.record()
+        hits = []
+        for s0 in range(0, nr, 64):
+            hits += index.search_arrays(recall_qs[s0:s0 + 64], n_cand=depth, top=TOP_K)
+        e1.record()
+        torch.cuda.synchronize()
+        depths.append(dict(recall(hits, depth),
+                           queries_per_s=round(nr / (e0.elapsed_time(e1) * 1e-3), 2)))
+    qps_l = len(qs) / (ms_learned * 1e-3)
+    qps_lr = nr / (ms_learned_r * 1e-3)
+    qps_e = nr / (ms_exact * 1e-3)
+    out = {
+        "metric": "queries/s of the learned prefilter at >= 0.99 recall of the exact top-1000",
+        "value": round(qps_l, 2), "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp8 e4m3 + int16x2",
+        "data": "synthetic",
+        "config": {"workload": "learned prefilter at its stated size",
+                   "db_sequences": n_seqs, "db_residues": int(n_res),
+                   "queries": len(qs), "recall_queries": nr,
+                   "planted_homologs_per_recall_query": int(args.recall_homologs),
+                   "identity": list(IDENT), "candidates_per_query": 32768, "top_k": TOP_K,
+                   "train_pairs": n_pairs, "train_epochs": args.learned_epochs},
+        "queries_per_s_recall_queries": round(qps_lr, 2),
+        "exact_queries_per_s": round(qps_e, 3),
+        "speedup_vs_exact": round(qps_lr / qps_e, 2),
+        "recall_of_exact_top1000": r32["recall_of_exact_top1000"],
+        "recall_min": r32["recall_min"],
+        "recall_by_identity_band": r32["recall_by_identity_band"],
+        "scores_equal_exact": all(d["scores_equal_exact"] for d in depths),
+        "candidate_depths": depths,
+        "train_loss_first_last": [hist["losses"][0][1], hist["losses"][-1][1]],
+        "train_steps": hist["steps"],
+        "seconds_build_db": round(t1 - t0, 1), "seconds_pairs": round(t2 - t1, 1),
+        "seconds_train": round(t3 - t2, 1), "seconds_index": round(t4 - t3, 1),
+        "ms_learned": round(ms_learned, 1), "ms_exact": round(ms_exact, 1),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def exact_saturation(db, n_q=16, n_batches=3, seed=7):
     """Saturation rate of the exact pipeline (``serve.GpuExecutor``: affine
     SW of every segment, top-k per batch) at this database size: ``n_q``
@@ -980,6 +1140,14 @@ def main():
     ap.add_argument("--serving-scale", type=int, default=0,
                     help="instead of the benchmark: build a database of this many sequences, "
                          "its learned index, and run the serving sweep over it")
+    ap.add_argument("--learned-scale", action="store_true",
+                    help="instead of the benchmark: the learned prefilter at its stated size "
+                         "(training on --learned-pairs pairs, --learned-queries timed queries, "
+                         "recall over --recall-queries queries with planted homologs)")
+    ap.add_argument("--recall-queries", type=int, default=128,
+                    help="queries with planted homologs whose recall --learned-scale reports")
+    ap.add_argument("--recall-homologs", type=int, default=500,
+                    help="planted homologs per recall query in --learned-scale")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -987,6 +1155,8 @@ def main():
         bench_reference(args)
     elif args.serving_scale > 0:
         bench_serving_scale(args)
+    elif args.learned_scale:
+        bench_learned_scale(args)
     else:
         bench_b200(args)
 

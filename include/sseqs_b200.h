@@ -331,7 +331,10 @@ int sseqs_gemm_bf16(int a_t, int b_t, int epilogue, int64_t M, int64_t N, int64_
  * epilogue is 1, 2, 3, 5 or 6; otherwise on mma.sync.  set_tensor_path(0)
  * forces mma.sync (1 restores the default).  gemm_error reads and clears the
  * flag a tcgen05 launch sets when one of its bounded waits ran out
- * (synchronous). */
+ * (synchronous).  A set flag means the tensor-core unit did not answer in
+ * time: the launch's output is invalid, and since its last operations were
+ * only waited for with a bound, the caller should treat the device state as
+ * suspect (stop issuing work and reset the context), not only that output. */
 int sseqs_gemm_set_tensor_path(int tcgen05);
 int sseqs_gemm_error(int* out);
 

@@ -79,10 +79,12 @@ def buckets(lengths) -> dict:
 
 @dataclass
 class QueryHits:
-    """Top-k of one query over the database: score desc, then (batch, segment)."""
+    """Top-k of one query over the database: score desc, then (batch, segment)
+    (or normalised score desc when searched with ``rank="norm"``)."""
     scores: np.ndarray      # int32
     batch: np.ndarray       # int32
     segment: np.ndarray     # int32 (delimiter-based segment index g)
+    norm: np.ndarray | None = None   # float32 score / sqrt(Lq * maxlen of the batch)
 
 
 class _Scratch:
@@ -170,7 +172,14 @@ class BatchedSearcher:
         self.plans: dict = {}
         self.scratch = _Scratch(db, self.group)
 
-    def search(self, queries) -> list[QueryHits]:
+    def search(self, queries, rank: str = "score") -> list[QueryHits]:
+        """Top-k per query over every batch: by affine score (``rank="score"``)
+        or by normalised score (``"norm"``: float32 score over float32
+        sqrt(Lq * maxlen of the hit's batch), the ranking of the exhaustive
+        search, sseqs/msa.py:339-345), ties by batch, then segment.  A
+        batch's own top-k is the same under both (one maxlen per batch)."""
+        if rank not in ("score", "norm"):
+            raise ValueError("rank is 'score' or 'norm'")
         if isinstance(queries, str):
             queries = [queries]
         db = self.db
@@ -193,7 +202,8 @@ class BatchedSearcher:
                                                         self.top_k, self.gaps, self.use_graphs)
                 plan.run([enc[i] for i in grp])
                 for j, qi in enumerate(grp):
-                    per_query[qi] = _collect(plan, j, self.top_k)
+                    per_query[qi] = _collect(plan, j, self.top_k,
+                                             lengths[qi] if rank == "norm" else None)
         return per_query
 
 
@@ -208,7 +218,7 @@ def search_queries(queries, db, *, top_k: int = 4096, gap_open: int = 11, gap_ex
                            use_graphs=use_graphs, autotune=autotune, group=group).search(queries)
 
 
-def _collect(plan: _GroupPlan, j: int, top_k: int) -> QueryHits:
+def _collect(plan: _GroupPlan, j: int, top_k: int, qlen: int | None = None) -> QueryHits:
     sc, bt, sg = [], [], []
     for bi, k in enumerate(plan.kb):
         if k <= 0 or plan.n[bi] <= 0:
@@ -221,5 +231,10 @@ def _collect(plan: _GroupPlan, j: int, top_k: int) -> QueryHits:
         z = np.zeros(0, dtype=np.int32)
         return QueryHits(z, z, z)
     sc, bt, sg = np.concatenate(sc), np.concatenate(bt), np.concatenate(sg)
-    order = np.lexsort((sg, bt, -sc.astype(np.int64)))[:top_k]
-    return QueryHits(sc[order], bt[order], sg[order])
+    if qlen is None:
+        order = np.lexsort((sg, bt, -sc.astype(np.int64)))[:top_k]
+        return QueryHits(sc[order], bt[order], sg[order])
+    ml = np.array([b.maxlen for b in plan.db.batches], dtype=np.int64)[bt]
+    norm = (sc.astype(np.float32) / np.sqrt((qlen * ml).astype(np.float32))).astype(np.float32)
+    order = np.lexsort((sg, bt, -norm.astype(np.float64)))[:top_k]
+    return QueryHits(sc[order], bt[order], sg[order], norm[order])

@@ -342,7 +342,9 @@ int launch_gemm(const GemmArgs& g, cudaStream_t stream, int splits = 1) {
 // SM's 512 tensor-memory columns); one thread issues the MMAs of a
 // stage (K 16 each) and commits them to the stage's mbarrier, which the
 // loaders wait on before reusing the stage.  Every wait is bounded: a
-// wait that runs out sets *err and the kernel stops issuing work.  The
+// wait that runs out sets *err, the kernel stops issuing work and waits
+// (bounded) for the MMAs it already issued before it frees the tensor
+// memory.  The
 // epilogue reads the accumulators with tcgen05.ld (warp w reads lanes
 // 32(w%4)..+31 = output rows, warps 0-3 columns 0-127 and warps 4-7
 // columns 128-255) and applies the same fused epilogues as the mma.sync
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int*
   // align the tile area to 1024 bytes
   const uint32_t raw = smem_u32(tsm);
   unsigned char* tiles = tsm + ((1024 - (raw & 1023)) & 1023);
-  __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+  __shared__ __align__(8) uint64_t mbar[TC_STAGES], drain;
   __shared__ uint32_t tmem_base_s;
   __shared__ int abort_s;
 
@@ -408,6 +410,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int*
   if (tid == 0) {
     for (int s = 0; s < TC_STAGES; ++s)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[s])), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&drain)), "r"(1));
     abort_s = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -493,7 +496,16 @@ __global__ void __launch_bounds__(TC_THREADS, 2) gemm_tc_kernel(GemmArgs g, int*
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
+    // MMAs already issued may still run: before the tensor memory and the
+    // stages are given up, wait (bounded) until every one of them is done
+    if (tid == 0) {
+      atomicExch(err, 1);
+      if (ktiles > 0) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(&drain)) : "memory");
+        mbar_wait(smem_u32(&drain), 0);
+      }
+    }
   } else {
     const int wq = warp & 3;                       // lanes 32*wq .. +31
     const int64_t m = m0 + wq * 32 + lane;
