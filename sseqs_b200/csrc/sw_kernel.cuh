@@ -9,9 +9,15 @@
 // any lane mapping.
 //
 // B200 mapping.  Two stripes of the same target share one 32-bit register as
-// int16x2 (lo = stripe 2m, hi = stripe 2m+1).  A lane holds W such words per
-// column, so a target occupies G = 32/(2W) lanes and a warp scores 2W
-// targets side by side.  The query profile (score of each residue class
+// int16x2: the lo halves carry stripes 0..15 and the hi halves stripes
+// 16..31 (word w of lane gl: stripes gl*W + w and 16 + gl*W + w).  A lane
+// holds W such words per column, so a target occupies G = 32/(2W) lanes and
+// a warp scores 2W targets side by side.  With this order a word's diagonal
+// input at its first column is the last column of the word before it, both
+// halves at once; only the first word of a lane takes it from the lane
+// before, and at lane 0 its hi half continues stripe 15 (the lo half of the
+// group's last lane) while its lo half is column -1 -- one shuffle and one
+// byte permute per row.  The query profile (score of each residue class
 // against every column, already packed as the lane's int16x2 words) sits in
 // shared memory; a lane fetches its row of it with 128-bit loads.
 //
@@ -330,8 +336,8 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       word = pack2(s0, s1);
     } else if (v < L::NWD) {
       const int w = v / TPT, k = v - w * TPT;
-      const int j = (gl * 2 * W + 2 * w) * TPT + k;
-      int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + TPT);
+      const int j = (gl * W + w) * TPT + k;             // stripe gl * W + w (lo), + 16 (hi)
+      int s0 = score_of(a.q, a.Lq, c, j), s1 = score_of(a.q, a.Lq, c, j + 16 * TPT);
       s0 = (s0 == kNeg) ? pad : (aff_tab ? s0 : s0 - gap);
       s1 = (s1 == kNeg) ? pad : (aff_tab ? s1 : s1 - gap);
       word = pack2(s0, s1);
@@ -347,6 +353,10 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   const int gl = lane - grp * G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
   const int leader = grp * G;
+  // diagonal input of a lane's first word: the lane before it (rotating
+  // inside the group); at lane 0 the lo half is column -1 instead
+  const int src_left = (gl + G - 1) % G;
+  const uint32_t sel_left = gl == 0 ? 0x1054u : 0x3210u;
 
   const uint32_t gap2 = pack2(gap, gap);       // linear gap, -16384 <= gap <= 0
   const uint32_t nopen2 = pack2(-open, -open); // affine -open, 0 <= open <= 16384
@@ -380,12 +390,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       const uint4 x = pr[v * L::VEC_STEP];
       s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
-    uint32_t from_left = __shfl_up_sync(0xffffffffu, SL[WL - 1][TPT - 1], 1, G);
-    if (gl == 0) from_left = gap2;                  // column -1 of stripe 0
     uint32_t din[WL];                               // diagonals, from the previous row
+    din[0] = __byte_perm(__shfl_sync(0xffffffffu, SL[WL - 1][TPT - 1], src_left, G), gap2,
+                         sel_left);                 // column -1 of stripe 0: H + gap = gap
 #pragma unroll
-    for (int w = 0; w < WL; ++w)
-      din[w] = __byte_perm(w == 0 ? from_left : SL[w - 1][TPT - 1], SL[w][TPT - 1], 0x5432);
+    for (int w = 1; w < WL; ++w) din[w] = SL[w - 1][TPT - 1];
     uint32_t pend = 0;
 #pragma unroll
     for (int w = 0; w < WL; ++w) {
@@ -438,14 +447,18 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
       const uint4 x = pr[v * L::VEC_STEP];
       s[4 * v] = x.x; s[4 * v + 1] = x.y; s[4 * v + 2] = x.z; s[4 * v + 3] = x.w;
     }
-    uint32_t from_left = __shfl_up_sync(0xffffffffu, SA[WA - 1][TPT - 1], 1, G);
-    if (gl == 0) from_left = 0u;                    // column -1 of stripe 0
     uint32_t din[WA];                               // diagonals, from the previous row
-#pragma unroll
-    for (int w = 0; w < WA; ++w) {
-      const uint32_t prev = w == 0 ? from_left : SA[w - 1][TPT - 1];
-      din[w] = PAIR ? prev : __byte_perm(prev, SA[w][TPT - 1], 0x5432);
+    if constexpr (PAIR) {
+      // both halves hold stripe gl * W + w: the lane before, 0 at lane 0
+      uint32_t from_left = __shfl_up_sync(0xffffffffu, SA[WA - 1][TPT - 1], 1, G);
+      if (gl == 0) from_left = 0u;                  // column -1 of stripe 0
+      din[0] = from_left;
+    } else {
+      din[0] = __byte_perm(__shfl_sync(0xffffffffu, SA[WA - 1][TPT - 1], src_left, G), 0u,
+                           sel_left);               // column -1 of stripe 0: D = 0
     }
+#pragma unroll
+    for (int w = 1; w < WA; ++w) din[w] = SA[w - 1][TPT - 1];
     uint32_t pend = 0;
 #pragma unroll
     for (int w = 0; w < WA; ++w) {
