@@ -197,6 +197,19 @@ int sseqs_topk(const void* keys, int key_type, int64_t n, int64_t k, int32_t* ou
 int sseqs_topk_static(const void* keys, int key_type, int64_t n, int64_t k, int32_t* out_idx,
                       cudaStream_t stream);
 
+/* Packs segments of several resident buffers into one: segment i, the
+ * len[i] bytes at byte src[i] of the buffer whose device address is
+ * bases[part[i]], is copied to out + dst[i] and followed by one '@' (the
+ * caller chooses dst so that segments do not overlap, e.g. the exclusive
+ * running sum of len + 1).  With delim[i] = dst[i] + len[i] the packed buffer
+ * is a database batch of its own whose segment i is segment i of the list,
+ * so candidates from many batches can be scored in one launch.  No
+ * reference counterpart (the reference scores one batch at a time,
+ * sseqs/msa.py:235). */
+int sseqs_pack_segments(const uint64_t* bases, const int32_t* part, const int64_t* src,
+                        const int32_t* len, const int64_t* dst, int64_t n, uint8_t* out,
+                        cudaStream_t stream);
+
 /* Hit strings of selected segments: row r of out (width bytes) receives
  * ascii[offsets[g] .. offsets[g] + min(width, lengths[g])), g = idx[r], the
  * rest of the row zero, and out_len[r] the copied length.  Replaces the

@@ -44,6 +44,7 @@ _SIGNATURES = {
     "sseqs_topk": (_I, [_P, _I, _I64, _I64, _P, _P, _SZ, _P]),
     "sseqs_topk_static": (_I, [_P, _I, _I64, _I64, _P, _P]),
     "sseqs_gather_windows": (_I, [_P, _P, _P, _P, _I64, _I, _P, _P, _P]),
+    "sseqs_pack_segments": (_I, [_P, _P, _P, _P, _P, _I64, _P, _P]),
     "sseqs_backtrack_workspace_bytes": (_SZ, [_I, _I, _I]),
     "sseqs_backtrack_affine": (_I, [_P, _I, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I,
                                     _P, _I, _P, _SZ, _P]),

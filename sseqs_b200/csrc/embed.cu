@@ -1427,18 +1427,30 @@ __global__ void __launch_bounds__(SEL_THREADS, 1)
               "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < a.n) {
+        // the 32 lanes are 32 rows of the same query column: per column one
+        // atomic reserves the slots of every lane that passes, and lane 0
+        // issues the atomics of all 16 columns back to back so that their
+        // latencies overlap
+        unsigned m[16];
+        int base[16] = {};
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const float s = __uint_as_float(v[j]);
-            const int c = c0 + j;
-            if (s >= tau_s[c]) {             // padding columns have tau = +inf
-              const int q = q0 + c;
-              const int slot = atomicAdd(a.count + q, 1);
-              if (slot < a.cap) {
-                a.cand[(int64_t)q * a.cap + slot] = row;
-                a.cand_score[(int64_t)q * a.cap + slot] = s;
-              }
+        for (int j = 0; j < 16; ++j)      // padding columns have tau = +inf
+          m[j] = __ballot_sync(0xffffffffu, row < a.n && __uint_as_float(v[j]) >= tau_s[c0 + j]);
+        if (lane == 0) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            base[j] = m[j] ? atomicAdd(a.count + q0 + c0 + j, __popc(m[j])) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          if (m[j] == 0) continue;                         // warp-uniform
+          const int b0 = __shfl_sync(0xffffffffu, base[j], 0);
+          if ((m[j] >> lane) & 1u) {
+            const int q = q0 + c0 + j;
+            const int slot = b0 + __popc(m[j] & ((1u << lane) - 1u));
+            if (slot < a.cap) {
+              a.cand[(int64_t)q * a.cap + slot] = row;
+              a.cand_score[(int64_t)q * a.cap + slot] = __uint_as_float(v[j]);
             }
           }
         }

@@ -491,6 +491,47 @@ extern "C" int sseqs_gather_windows(const uint8_t* ascii, const int64_t* offsets
   return status_of(cudaGetLastError());
 }
 
+// ------------------------------------------------------ segment packing
+// Segment i (bytes [src[i], src[i] + len[i]) of the buffer bases[part[i]])
+// goes to out[dst[i] ..], followed by one '@'.  One warp per segment: the
+// bytes are moved as 4-byte words where source and destination share their
+// alignment, else byte by byte.
+__global__ void pack_segments_kernel(const uint64_t* bases, const int32_t* part,
+                                     const int64_t* src, const int32_t* len, const int64_t* dst,
+                                     int64_t n, uint8_t* out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(bases[part[i]]) + src[i];
+    uint8_t* d = out + dst[i];
+    const int L = len[i];
+    const int head = (int)((4 - (reinterpret_cast<uintptr_t>(d) & 3)) & 3);
+    if (((reinterpret_cast<uintptr_t>(s) ^ reinterpret_cast<uintptr_t>(d)) & 3) == 0 && L > head) {
+      if (lane < head) d[lane] = s[lane];
+      const int words = (L - head) >> 2;
+      const uint32_t* sw = reinterpret_cast<const uint32_t*>(s + head);
+      uint32_t* dw = reinterpret_cast<uint32_t*>(d + head);
+      for (int w = lane; w < words; w += 32) dw[w] = sw[w];
+      for (int b = head + 4 * words + lane; b < L; b += 32) d[b] = s[b];
+    } else {
+      for (int b = lane; b < L; b += 32) d[b] = s[b];
+    }
+    if (lane == 0) d[L] = 64;
+  }
+}
+
+extern "C" int sseqs_pack_segments(const uint64_t* bases, const int32_t* part, const int64_t* src,
+                                   const int32_t* len, const int64_t* dst, int64_t n, uint8_t* out,
+                                   cudaStream_t stream) {
+  if (n < 0) return SSEQS_ERR_ARG;
+  if (n == 0) return SSEQS_OK;
+  if (!bases || !part || !src || !len || !dst || !out) return SSEQS_ERR_ARG;
+  const int grid = (int)std::min<int64_t>((n + 7) / 8, (int64_t)device_sm_count() * 16);
+  { pack_segments_kernel<<<grid, 256, 0, stream>>>(bases, part, src, len, dst, n, out);
+    count_launches(1); }
+  return status_of(cudaGetLastError());
+}
+
 // ------------------------------------------------ top-k without allocation
 // Scratch of sseqs_topk_static: the same control block and per-tile counters
 // as sseqs_topk's workspace, in a fixed array that every GPU loading this

@@ -591,6 +591,7 @@ class LearnedIndex:
             dev = self.db.device
             bs = self.db.batches
             seg = [b.seg_index[:b.n_segments].to(torch.int32) for b in bs]
+            nd = [b.delim.numel() for b in bs]
             self._tabs = {
                 "cum": torch.from_numpy(self.cum).to(dev),
                 "nseg": torch.tensor([b.n_segments for b in bs] or [0], dtype=torch.int64,
@@ -600,8 +601,20 @@ class LearnedIndex:
                 # segment number of every index row (the delimiter-based index
                 # the exhaustive search reports)
                 "seg": torch.cat(seg) if seg else torch.zeros(1, dtype=torch.int32, device=dev),
+                # every batch's '@' positions, one after another, and where
+                # each batch's begin; the batches' device addresses
+                "delim": torch.cat([b.delim for b in bs]) if bs else
+                         torch.zeros(1, dtype=torch.int32, device=dev),
+                "doff": torch.tensor(np.concatenate([[0], np.cumsum(nd)[:-1]]) if nd else [0],
+                                     dtype=torch.int64, device=dev),
+                "bases": torch.tensor([b.ascii.data_ptr() for b in bs] or [0],
+                                      dtype=torch.int64, device=dev),
             }
         return self._tabs
+
+    # packed candidate bytes per rescoring call, at most (segment windows are
+    # addressed with int32 delimiter positions)
+    PACK_LIMIT = 1_500_000_000
 
     def rescore_flat(self, queries, qid: torch.Tensor, rows: torch.Tensor, top: int = 4096,
                      gap_open=11, gap_extend=1) -> list:
@@ -612,11 +625,14 @@ class LearnedIndex:
         ``(norm float32, batch, segment, affine int64)`` sorted by normalised
         score desc, then batch, then segment.
 
-        The work per engine step does not grow with the number of database
-        batches beyond one SW launch per (batch, stripe-width group): the
-        target lists, their positions and the ranking are built with a fixed
-        number of whole-array operations, and the hits come back in one copy
-        per field."""
+        The distinct candidate segments of all queries, from whatever
+        batches they lie in, are first packed into one '@'-separated buffer
+        (``sseqs_pack_segments``), so every stripe-width group of queries is
+        scored by one SW launch over all its candidates whatever the number
+        of database batches; a segment scores the same there as in its batch
+        (the same bytes, the same skip).  The target rows, their positions
+        and the ranking are built with a fixed number of whole-array
+        operations, and the hits come back in one copy per field."""
         from . import batched
         sw = importlib.import_module("sseqs_b200.sw")
         dev = self.db.device
@@ -626,54 +642,78 @@ class LearnedIndex:
         if nq == 0 or rows.numel() == 0 or nb == 0:
             return [empty for _ in range(nq)]
         T = self._batch_tables()
-        enc = [sw.encode_query(q, device=dev) for q in queries]
-        lens = [e.numel() for e in enc]
         batch = torch.searchsorted(T["cum"][1:], rows, right=True)
         local = rows - T["cum"][batch]
         ok = (local >= 1) & (local <= T["nseg"][batch] - 2)
         qid, rows, batch = qid[ok], rows[ok], batch[ok]
-        seg = T["seg"][rows]
         n = qid.numel()
         if n == 0:
             return [empty for _ in range(nq)]
-        # candidates per (query, batch): contiguous runs of the flat order
-        cqb = to_host(torch.bincount(qid * nb + batch, minlength=nq * nb)).reshape(nq, nb)
-        cqb = cqb.astype(np.int64)
-        start = (np.cumsum(cqb.reshape(-1)) - cqb.reshape(-1)).reshape(nq, nb)
-        # launches: per batch, per stripe width, up to GROUP queries; every
-        # query row of a launch holds its own targets, padded with its last
+        seg = T["seg"][rows]
+        # the distinct candidate segments and their windows (segment g of a
+        # batch: bytes delim[g-1] + 1 .. delim[g]; every candidate has g >= 1)
+        urows, inv = torch.unique(rows, return_inverse=True)
+        ub = torch.searchsorted(T["cum"][1:], urows, right=True)
+        dpos = T["doff"][ub] + T["seg"][urows].to(torch.int64)
+        end = T["delim"][dpos].to(torch.int64)
+        start = T["delim"][dpos - 1].to(torch.int64) + 1
+        ulen = end - start
+        dst = torch.cumsum(ulen + 1, 0) - (ulen + 1)
+        per_q = to_host(torch.bincount(qid, minlength=nq)).astype(np.int64)
+        total = int((dst[-1] + ulen[-1] + 1).item())
+        if total > self.PACK_LIMIT and nq > 1:
+            # too many bytes for one packed buffer: score the queries in two halves
+            h = nq // 2
+            cut = int(per_q[:h].sum())
+            lo = self.rescore_flat(queries[:h], qid[:cut], rows[:cut], top, gap_open, gap_extend)
+            hi = self.rescore_flat(queries[h:], qid[cut:] - h, rows[cut:], top, gap_open,
+                                   gap_extend)
+            return lo + hi
+        if total > self.PACK_LIMIT:
+            raise ValueError("candidate segments of one query exceed the packing limit")
+        packed = torch.empty(total, dtype=torch.uint8, device=dev)
+        # the int32 copies are held by names until the launch has been queued
+        # (a temporary freed earlier could hand its memory to the next one)
+        ub32, ulen32 = ub.to(torch.int32), ulen.to(torch.int32)
+        check(lib().sseqs_pack_segments(ptr(T["bases"]), ptr(ub32), ptr(start), ptr(ulen32),
+                                        ptr(dst), urows.numel(), ptr(packed), stream_ptr()),
+              "pack_segments")
+        pdelim = (dst + ulen).to(torch.int32)
+        enc = [sw.encode_query(q, device=dev) for q in queries]
+        lens = [e.numel() for e in enc]
+        qstart_h = np.cumsum(per_q) - per_q
+        # one launch per stripe-width group of up to GROUP queries; every
+        # query row holds its own targets (indices into the packed buffer),
+        # padded with its last one
         plan, pos_parts, qid_parts = [], [], []
         pos_off = q_off = 0
-        bk = batched.buckets(lens)
-        for bi in range(nb):
-            for tpt, members in bk.items():
-                live_q = [q for q in members if cqb[q, bi] > 0]
-                for s0 in range(0, len(live_q), batched.GROUP):
-                    grp = live_q[s0:s0 + batched.GROUP]
-                    cnt = cqb[grp, bi]
-                    m = int(cnt.max())
-                    k = np.minimum(np.arange(m)[None, :], cnt[:, None] - 1)
-                    pos_parts.append((start[grp, bi][:, None] + k).reshape(-1))
-                    qid_parts.append(np.asarray(grp, np.int64))
-                    plan.append((bi, tpt, len(grp), m, pos_off, q_off))
-                    pos_off += len(grp) * m
-                    q_off += len(grp)
+        for tpt, members in batched.buckets(lens).items():
+            live_q = [q for q in members if per_q[q] > 0]
+            for s0 in range(0, len(live_q), batched.GROUP):
+                grp = live_q[s0:s0 + batched.GROUP]
+                cnt = per_q[grp]
+                m = int(cnt.max())
+                k = np.minimum(np.arange(m)[None, :], cnt[:, None] - 1)
+                pos_parts.append((qstart_h[grp][:, None] + k).reshape(-1))
+                qid_parts.append(np.asarray(grp, np.int64))
+                plan.append((tpt, len(grp), m, pos_off, q_off))
+                pos_off += len(grp) * m
+                q_off += len(grp)
         pos = torch.from_numpy(np.concatenate(pos_parts)).to(dev)
         lq = torch.from_numpy(np.concatenate(qid_parts)).to(dev)
-        idx_all = seg[pos]
+        idx_all = inv[pos].to(torch.int32)
         qbuf = torch.zeros((nq, batched.MAX_QUERY), dtype=torch.uint8, device=dev)
         for j, e in enumerate(enc):
             qbuf[j, :e.numel()] = e
         qlen = torch.tensor(lens, dtype=torch.int32, device=dev)
         qrows, qls = qbuf[lq], qlen[lq]
         aff = torch.empty(n, dtype=torch.int32, device=dev)
-        for bi, tpt, G, m, po, qo in plan:
-            b = self.db.batches[bi]
-            sc = batched.sw_scan_queries(qrows[qo:qo + G], qls[qo:qo + G], tpt, b.ascii,
-                                         b.delim, affine=True,
-                                         good_idx=idx_all[po:po + G * m].view(G, m), skip=1,
-                                         gap_a=gap_open, gap_b=gap_extend)
+        for tpt, G, m, po, qo in plan:
+            sc = batched.sw_scan_queries(qrows[qo:qo + G], qls[qo:qo + G], tpt, packed, pdelim,
+                                         affine=True, good_idx=idx_all[po:po + G * m].view(G, m),
+                                         skip=1, gap_a=gap_open, gap_b=gap_extend)
             aff.index_copy_(0, pos[po:po + G * m], sc[:, :m].reshape(-1))
+        del packed
         # normalised score as the exhaustive search forms it (float32 of the
         # affine score over float32 sqrt of Lq * maxlen of the hit's batch)
         den = torch.sqrt((qlen.to(torch.int64)[qid] * T["maxlen"][batch]).to(torch.float32))
@@ -682,8 +722,7 @@ class LearnedIndex:
         # (batch, segment) ascending, which the stable sorts keep for ties
         o = torch.sort(norm, descending=True, stable=True).indices
         o = o[torch.sort(qid[o], stable=True).indices]
-        per_q = cqb.sum(1)
-        qstart = torch.from_numpy(np.cumsum(per_q) - per_q).to(dev)
+        qstart = torch.from_numpy(qstart_h).to(dev)
         rank = torch.arange(n, device=dev) - qstart[qid[o]]
         o = o[rank < top]
         keep = np.minimum(per_q, top)

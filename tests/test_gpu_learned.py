@@ -380,6 +380,11 @@ def test_rescore_matches_direct_scoring():
         for _ in queries]
     top = 150
     got = idx.rescore(queries, cands, top=top)
+    # the same with the packed buffer limited so that the queries are scored
+    # in several parts
+    idx.PACK_LIMIT = 150_000
+    assert idx.rescore(queries, cands, top=top) == got
+    del idx.PACK_LIMIT
     for j, q in enumerate(queries):
         enc = sw.encode_query(q)
         rows = cands[j].cpu().numpy()
