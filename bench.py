@@ -323,7 +323,7 @@ def serving_leg(db, n_requests, rate, seed=4, index=None):
             "lengths": "U(50, 1000), seed %d" % seed}
 
 
-def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
+def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5, target_power=0.5):
     """Learned prefilter: train the conv embedder on ``n_pairs`` seeded
     (query, target) pairs labelled by this package's exact SW, embed every
     database segment into FP8 codes, then per query take 32768 candidates by
@@ -340,7 +340,7 @@ def learned_leg(db, exact_rows, n_pairs, n_queries, epochs=1, seed=5):
     torch.cuda.synchronize()
     t1 = time.time()
     model = learned.Embedder(seed=seed)
-    hist = learned.train(model, pairs, epochs=epochs, seed=seed)
+    hist = learned.train(model, pairs, epochs=epochs, seed=seed, target_power=target_power)
     torch.cuda.synchronize()
     t2 = time.time()
     index = learned.LearnedIndex(model, db)
@@ -572,7 +572,8 @@ def bench_learned_scale(args):
     pairs = learned.training_pairs(max(1, args.learned_pairs // 256), 256, seed=5)
     t2 = time.time()
     model = learned.Embedder(seed=5)
-    hist = learned.train(model, pairs, epochs=args.learned_epochs, seed=5)
+    hist = learned.train(model, pairs, epochs=args.learned_epochs, seed=5,
+                         target_power=args.learned_target_power)
     n_pairs = int(pairs.y.numel())
     del pairs
     torch.cuda.empty_cache()
@@ -670,7 +671,8 @@ def bench_learned_scale(args):
                    "queries": len(qs), "recall_queries": nr,
                    "planted_homologs_per_recall_query": int(args.recall_homologs),
                    "identity": list(IDENT), "candidates_per_query": 32768, "top_k": TOP_K,
-                   "train_pairs": n_pairs, "train_epochs": args.learned_epochs},
+                   "train_pairs": n_pairs, "train_epochs": args.learned_epochs,
+                   "train_target_power": args.learned_target_power},
         "queries_per_s_recall_queries": round(qps_lr, 2),
         "exact_queries_per_s": round(qps_e, 3),
         "speedup_vs_exact": round(qps_lr / qps_e, 2),
@@ -749,7 +751,8 @@ def bench_serving_scale(args):
     t1 = time.time()
     pairs = learned.training_pairs(max(1, args.learned_pairs // 256), 256, seed=5)
     model = learned.Embedder(seed=5)
-    learned.train(model, pairs, epochs=args.learned_epochs, seed=5)
+    learned.train(model, pairs, epochs=args.learned_epochs, seed=5,
+                  target_power=args.learned_target_power)
     del pairs
     torch.cuda.empty_cache()
     t2 = time.time()
@@ -1006,7 +1009,8 @@ def bench_b200(args):
         out["serving"] = serving_leg(db, args.serve_requests, args.serve_rate)
     if world == 1 and args.learned_pairs > 0:
         out["learned"] = learned_leg(db, exact_rows, args.learned_pairs, args.learned_queries,
-                                     epochs=args.learned_epochs)
+                                     epochs=args.learned_epochs,
+                                     target_power=args.learned_target_power)
         out["learned"]["speedup_vs_exact_step"] = round(
             out["learned"]["queries_per_s"] / out["queries_per_s"], 2)
         if args.serve_requests > 0:
@@ -1136,6 +1140,9 @@ def main():
                     help="queries timed in the learned-prefilter leg")
     ap.add_argument("--learned-epochs", type=int, default=2,
                     help="training epochs over the learned leg's pairs")
+    ap.add_argument("--learned-target-power", type=float, default=0.5,
+                    help="the embedder's training target is the normalised SW score to this "
+                         "power (below 1 spreads remote homologs from unrelated pairs)")
     ap.add_argument("--sweep-seconds", type=float, default=4.0,
                     help="seconds of Poisson arrivals per rate of the learned serving sweep "
                          "(rates %s q/s); 0 skips it" % (SWEEP_RATES,))
