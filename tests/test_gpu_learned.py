@@ -431,3 +431,33 @@ def test_candidates_take_top_keys_with_lower_rows_at_ties():
         mine = kr[kq == j]
         assert counts[j] == n_cand
         assert np.array_equal(mine, want)
+
+
+def test_pack_segments_copies_every_window():
+    """sseqs_pack_segments against a host copy: windows of 0..70 bytes from
+    three buffers at every source/destination alignment (the 4-byte-word and
+    the byte-by-byte paths), each followed by one '@'."""
+    from sseqs_b200 import _lib
+    rng = np.random.default_rng(9)
+    bufs = [torch.from_numpy(rng.integers(65, 90, size=n, dtype=np.uint8)).cuda()
+            for n in (1000, 777, 4096)]
+    n = 600
+    part = rng.integers(0, 3, n)
+    ln = rng.integers(0, 71, n)
+    ln[:6] = [0, 1, 2, 3, 4, 5]
+    src = np.array([rng.integers(0, bufs[p].numel() - l + 1) for p, l in zip(part, ln)])
+    dst = np.cumsum(ln + 1) - (ln + 1)
+    total = int(dst[-1] + ln[-1] + 1)
+    out = torch.full((total,), 0, dtype=torch.uint8, device="cuda")
+    bases = torch.tensor([b.data_ptr() for b in bufs], dtype=torch.int64, device="cuda")
+    part_d = torch.from_numpy(part.astype(np.int32)).cuda()
+    src_d = torch.from_numpy(src.astype(np.int64)).cuda()
+    len_d = torch.from_numpy(ln.astype(np.int32)).cuda()
+    dst_d = torch.from_numpy(dst.astype(np.int64)).cuda()
+    _lib.check(_lib.lib().sseqs_pack_segments(bases.data_ptr(), part_d.data_ptr(),
+                                              src_d.data_ptr(), len_d.data_ptr(),
+                                              dst_d.data_ptr(), n, out.data_ptr(), 0), "pack")
+    host = [b.cpu().numpy() for b in bufs]
+    want = np.concatenate([np.concatenate([host[p][s:s + l], [64]]).astype(np.uint8)
+                           for p, s, l in zip(part, src, ln)])
+    assert np.array_equal(out.cpu().numpy(), want)
