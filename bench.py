@@ -824,6 +824,60 @@ def cpu_sample_gcups(queries, budget_s, seed=0):
         f"({int(cells)} residue-columns x 2 variants) of a same-distribution database", dt
 
 
+def config1_leg(M, reps=20):
+    """The benchmark's CPU-runnable configuration: one query of 200 residues
+    (seed 0) against 100k synthetic sequences (same length model, 1% planted
+    homologs at 30-90% identity), exact linear (-1) + affine (11/1) search,
+    top 100 with alignments.  The GPU path (``msa.search`` + traceback, CUDA
+    events over ``reps`` searches) beside the CPU oracle on all host threads
+    over the same decoded database, both counted in SW cell updates of the
+    two variants."""
+    import torch
+    from oracle import oracle as O
+    from sseqs_b200 import dbtools
+    from sseqs_b200.database import Database
+    from sseqs_b200.to_a3m import traceback_all
+    q = dbtools.random_query(200, 0)
+    cb = 25_000_000                      # one chunk holds the ~30M residues
+    syn = dbtools.synthetic_db([q], 100_000, 0.01, (0.30, 0.90), seed=0, device="cuda",
+                               chunk_bytes=cb)
+    chunk = syn.chunks[0]
+    db = Database(syn.chunks, bs=cb)
+    del syn
+    cells = 2 * len(q) * segment_cells(db)
+
+    def once():
+        rows = M.search([q], db, num_msas=100, top_fft=1, top_sw=1, top_sw_affine=100)[0]
+        traceback_all(q, [r[5] for r in rows])
+
+    once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        once()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    a = O.xbit_decompress(chunk.cpu().numpy(), chunk.numel() * 8 // 5, 0)
+    seg = O.segment(a)
+    d = np.flatnonzero(a == 64).astype(np.int32)
+    good = np.arange(1, len(seg["lengths"]) - 1, dtype=np.int32)
+    cpu_cells = 2 * len(q) * float(seg["lengths"][1:-1].sum())
+    qi = O.encode_query(q)
+    nt = os.cpu_count() or 1
+    t0 = time.time()
+    O.sw_linear(qi, good, a, d, -1, nt)
+    O.sw_affine(qi, good, a, d + 1, 11, 1, nt)
+    dt = time.time() - t0
+    return {"workload": "1 query of 200 residues vs 100k sequences, exact linear + affine, "
+                        "top 100 with alignments",
+            "gpu_ms_per_query": round(ms, 2), "gpu_gcups": round(cells / (ms * 1e-3) / 1e9, 1),
+            "cpu_seconds": round(dt, 2), "cpu_gcups": round(cpu_cells / dt / 1e9, 3),
+            "cpu_cores": nt, "cpu_kind": "port",
+            "gpu_over_cpu": round((cells / (ms * 1e-3)) / (cpu_cells / dt), 1)}
+
+
 def bench_b200(args):
     import torch
     import torch.distributed as dist
@@ -1025,6 +1079,7 @@ def bench_b200(args):
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
                                "kind": "port", "sample": sample, "seconds": round(dt, 1)}
+        out["config1"] = config1_leg(M)
     print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
