@@ -824,8 +824,8 @@ def cpu_sample_gcups(queries, budget_s, seed=0):
         f"({int(cells)} residue-columns x 2 variants) of a same-distribution database", dt
 
 
-def config1_leg(M, reps=20):
-    """The benchmark's CPU-runnable configuration: one query of 200 residues
+def small_exact_leg(M, reps=20):
+    """The CPU-runnable exact search: one query of 200 residues
     (seed 0) against 100k synthetic sequences (same length model, 1% planted
     homologs at 30-90% identity), exact linear (-1) + affine (11/1) search,
     top 100 with alignments.  The GPU path (``msa.search`` + traceback, CUDA
@@ -1079,7 +1079,7 @@ def bench_b200(args):
         v, cores, sample, dt = cpu_sample_gcups(queries, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(v, 3), "unit": "GCUPS", "cores": cores,
                                "kind": "port", "sample": sample, "seconds": round(dt, 1)}
-        out["config1"] = config1_leg(M)
+        out["exact_q200_100k"] = small_exact_leg(M)
     print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
