@@ -1185,8 +1185,9 @@ def main():
                     help="queries of the batched uneven-length leg; 0 skips it")
     ap.add_argument("--serve-requests", type=int, default=24,
                     help="requests of the serving leg; 0 skips it")
-    ap.add_argument("--serve-rate", type=float, default=1.5,
-                    help="Poisson arrival rate (queries/s) of the serving leg")
+    ap.add_argument("--serve-rate", type=float, default=0.8,
+                    help="Poisson arrival rate (queries/s) of the serving leg (the exact "
+                         "pipeline serves about 1.2 q/s at 20M sequences)")
     ap.add_argument("--serve-rate-learned", type=float, default=10.0,
                     help="Poisson arrival rate (queries/s) of the learned serving leg")
     ap.add_argument("--learned-pairs", type=int, default=1_000_000,
