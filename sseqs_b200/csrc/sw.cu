@@ -84,13 +84,17 @@ const Tables& tables() {
     register_17_32(t);
     register_33_48(t);
     register_49_64(t);
+    register_1_16_def(t);
+    register_17_32_def(t);
+    register_33_48_def(t);
+    register_49_64_def(t);
   });
   return t;
 }
 
 struct Cache {
   std::mutex mu;
-  int max_blocks[2][kModes][64][64] = {};  // [variant][mode][TPT-1][device]
+  int max_blocks[2][2][kModes][64][64] = {};  // [gaps][variant][mode][TPT-1][device]
   int variant[kModes][64] = {};            // chosen variant per [mode][TPT-1]
   bool pairing[64] = {};                   // per [TPT-1]: batched affine launches pair queries
 };
@@ -118,6 +122,14 @@ unsigned int* ticket_slot(int dev) {
   return base[dev] + (next[dev]++ % kTicketSlots);
 }
 
+// Whether a launch of `mode` passes msa()'s gap parameters, so that the
+// kernel twin with those as constants (DEF) scores it.
+bool default_gaps(int mode, const SwArgs& a) {
+  if (mode == kLin) return a.p0 == kDefGap;
+  if (mode == kBoth) return a.p0 == kDefGap && a.p1 == kDefOpen && a.p2 == kDefExt;
+  return a.p0 == kDefOpen && a.p1 == kDefExt;   // kAff, kPair
+}
+
 // Launches the streaming kernel for one query (qt == nullptr; target
 // counter from the ring) or for the qt->n queries of a table (counters
 // a.ticket[0 .. qt->n), provided by the caller).
@@ -125,13 +137,14 @@ int launch_stream(SwArgs a, int mode, const QueryTable* qt, cudaStream_t stream)
   const int tpt = (a.Lq + 31) / 32;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return SSEQS_ERR_CUDA;
+  const int gaps = default_gaps(mode, a) ? 1 : 0;
   int blocks_per_sm, var;
   const KernelInfo* kp;
   {
     std::lock_guard<std::mutex> lk(cache().mu);
     var = cache().variant[mode][tpt - 1];
-    kp = &tables().k[var][mode][tpt - 1];
-    int& mb = cache().max_blocks[var][mode][tpt - 1][dev];
+    kp = &tables().k[gaps][var][mode][tpt - 1];
+    int& mb = cache().max_blocks[gaps][var][mode][tpt - 1][dev];
     if (mb == 0) {
       if (cudaFuncSetAttribute((const void*)kp->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kp->smem) != cudaSuccess)
@@ -429,5 +442,5 @@ extern "C" int sseqs_sw_get_variant(int affine, int tpt) {
 
 extern "C" int sseqs_sw_variant_words(int affine, int tpt, int wide) {
   if (tpt < 1 || tpt > 64 || (wide != 0 && wide != 1) || affine < 0 || affine >= kModes) return -1;
-  return tables().k[wide][affine][tpt - 1].words;
+  return tables().k[0][wide][affine][tpt - 1].words;
 }

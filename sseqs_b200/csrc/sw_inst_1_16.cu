@@ -1,12 +1,12 @@
-// Instantiations of the score kernel for stripe widths 1..16 (split across
-// translation units so that they compile in parallel).
+// Instantiations of the score kernel for stripe widths 1..16 with the gap
+// parameters read from the arguments (split across translation units so
+// that they compile in parallel).
 #include "sw_kernel.cuh"
 
 namespace sseqs {
 namespace sw {
 void register_1_16(Tables& t) {
   fill_range<1, false>(t, std::make_integer_sequence<int, 16>{});
-  fill_range<1, true>(t, std::make_integer_sequence<int, 16>{});
 }
 }  // namespace sw
 }  // namespace sseqs

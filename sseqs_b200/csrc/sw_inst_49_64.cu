@@ -1,12 +1,12 @@
-// Instantiations of the score kernel for stripe widths 49..64 (split across
-// translation units so that they compile in parallel).
+// Instantiations of the score kernel for stripe widths 49..64 with the gap
+// parameters read from the arguments (split across translation units so
+// that they compile in parallel).
 #include "sw_kernel.cuh"
 
 namespace sseqs {
 namespace sw {
 void register_49_64(Tables& t) {
   fill_range<49, false>(t, std::make_integer_sequence<int, 16>{});
-  fill_range<49, true>(t, std::make_integer_sequence<int, 16>{});
 }
 }  // namespace sw
 }  // namespace sseqs

@@ -244,7 +244,17 @@ struct Shape {
                         est_regs <= 170 ? 3 : 1);
 };
 
-template <int TPT, int W, int MODE>
+// The gap parameters msa() always passes (sseqs/msa.py:317, 331-332):
+// linear gap -1, affine open 11 and extend 1.  Every kernel has a twin
+// (DEF = true) with these as compile-time constants, picked by the host
+// whenever a call passes them; the int16x2 gap words then reach the DPX
+// instructions as immediates instead of registers.  Measured on B200 (1M
+// segments, widths 2-32): the affine kernel 5-16% faster (8% at most
+// widths) with scores unchanged; gap words passed as pre-packed kernel
+// parameters instead were 0-7% slower.
+constexpr int kDefGap = -1, kDefOpen = 11, kDefExt = 1;
+
+template <int TPT, int W, int MODE, bool DEF>
 __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MODE>::min_blocks)
     sw_stream_kernel(SwArgs a, const QueryTable qt) {
   constexpr bool PAIR = MODE == kPair;
@@ -307,11 +317,11 @@ __global__ void __launch_bounds__(Shape<TPT, W, MODE>::threads, Shape<TPT, W, MO
   uint8_t* lut = reinterpret_cast<uint8_t*>(prof + NTAB * kNumCls * L::CLS);
 
   // Gap parameters: linear gap (p0); affine open and extend (p0, p1 in the
-  // affine kernel; p1, p2 in the fused one).
-  const int gap = a.p0;
+  // affine kernel; p1, p2 in the fused one); constants in the DEF twin.
+  const int gap = DEF ? kDefGap : a.p0;
   constexpr bool AFF_ONLY = MODE == kAff || MODE == kPair;   // affine gaps in p0, p1
-  const int open = AFF_ONLY ? a.p0 : a.p1;
-  const int ext = AFF_ONLY ? a.p1 : a.p2;
+  const int open = DEF ? kDefOpen : AFF_ONLY ? a.p0 : a.p1;
+  const int ext = DEF ? kDefExt : AFF_ONLY ? a.p1 : a.p2;
 
   // Profile words.  Affine: s (real columns), -32768 + open (padding), so
   // that M' - open never leaves int16.  Linear: s - gap (the state carries
@@ -684,11 +694,11 @@ struct KernelInfo {
   int words = 0;
 };
 
-template <int TPT, int MODE, bool WIDE>
+template <int TPT, int MODE, bool WIDE, bool DEF>
 KernelInfo make_info() {
   constexpr int W = words_for<TPT, WIDE, MODE>();
   KernelInfo k;
-  k.fn = sw_stream_kernel<TPT, W, MODE>;
+  k.fn = sw_stream_kernel<TPT, W, MODE, DEF>;
   using L = Layout<TPT, W, vector_major<TPT, W, MODE>(), MODE == kPair>;
   k.smem = L::smem + (MODE == kBoth ? L::smem - 256 : 0);
   k.threads = Shape<TPT, W, MODE>::threads;
@@ -697,8 +707,10 @@ KernelInfo make_info() {
   return k;
 }
 
-// tables[variant][mode][TPT - 1], variant 0 = narrow, 1 = wide;
-// mode kLin, kAff or kBoth.  The fused kernel exists up to kMaxFusedTpt;
+// tables[gaps][variant][mode][TPT - 1]: gaps 0 = gap parameters read from
+// the arguments, 1 = the DEF twin (kDefGap, kDefOpen, kDefExt); variant 0 =
+// narrow, 1 = wide; mode kLin, kAff, kBoth or kPair.  The fused kernel
+// exists up to kMaxFusedTpt;
 // wider queries run the two kernels one after the other (fn == nullptr
 // here).  Measured on B200 (300k-1M segments), the fused pass beat the two
 // kernels by 4-17% up to width 16 and by 5% at 20 (8 rows per fetch),
@@ -706,27 +718,48 @@ KernelInfo make_info() {
 // registers there, which leaves 8 warps per SM.
 constexpr int kMaxFusedTpt = 21;
 struct Tables {
-  KernelInfo k[2][kModes][64];
+  KernelInfo k[2][2][kModes][64];
 };
 
-template <int T, bool WIDE>
+// Instantiations whose DEF twin spills under the register cap (ptxas, 4-8
+// bytes) where the runtime-gap kernel does not: their DEF slot holds the
+// runtime-gap kernel.
+template <int T, int MODE, bool WIDE>
+constexpr bool def_twin() {
+  return !(MODE == kLin && ((T == 15 && !WIDE) || (T == 23 && WIDE))) &&
+         !(MODE == kAff && T == 2 && !WIDE);
+}
+
+template <int T, int MODE, bool WIDE, bool DEF>
+KernelInfo make_slot() {
+  return make_info<T, MODE, WIDE, DEF && def_twin<T, MODE, WIDE>()>();
+}
+
+template <int T, bool WIDE, bool DEF>
 void fill_one(Tables& t) {
-  t.k[WIDE][kLin][T - 1] = make_info<T, kLin, WIDE>();
-  t.k[WIDE][kAff][T - 1] = make_info<T, kAff, WIDE>();
-  if constexpr (T <= kMaxFusedTpt) t.k[WIDE][kBoth][T - 1] = make_info<T, kBoth, WIDE>();
-  t.k[WIDE][kPair][T - 1] = make_info<T, kPair, WIDE>();
+  KernelInfo(&row)[kModes][64] = t.k[DEF][WIDE];
+  row[kLin][T - 1] = make_slot<T, kLin, WIDE, DEF>();
+  row[kAff][T - 1] = make_slot<T, kAff, WIDE, DEF>();
+  if constexpr (T <= kMaxFusedTpt) row[kBoth][T - 1] = make_slot<T, kBoth, WIDE, DEF>();
+  row[kPair][T - 1] = make_slot<T, kPair, WIDE, DEF>();
 }
 
-template <int LO, bool WIDE, int... I>
+template <int LO, bool DEF, int... I>
 void fill_range(Tables& t, std::integer_sequence<int, I...>) {
-  (fill_one<LO + I, WIDE>(t), ...);
+  (fill_one<LO + I, false, DEF>(t), ...);
+  (fill_one<LO + I, true, DEF>(t), ...);
 }
 
-// Defined in the instantiation units sw_inst_*.cu.
+// Defined in the instantiation units sw_inst_*.cu (runtime gaps) and
+// sw_inst_*_def.cu (the DEF twins).
 void register_1_16(Tables& t);
 void register_17_32(Tables& t);
 void register_33_48(Tables& t);
 void register_49_64(Tables& t);
+void register_1_16_def(Tables& t);
+void register_17_32_def(Tables& t);
+void register_33_48_def(Tables& t);
+void register_49_64_def(Tables& t);
 
 }  // namespace sw
 }  // namespace sseqs

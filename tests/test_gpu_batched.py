@@ -124,12 +124,14 @@ PAIR_LENGTHS = [1, 17, 33, 64, 65, 100, 129, 200, 257, 300, 416, 500, 545, 640, 
                 1000, 1024, 1100, 1500, 1800, 2048]
 
 
+@pytest.mark.parametrize("gaps", [(11, 1), (5, 2)], ids=["msa_gaps", "other_gaps"])
 @pytest.mark.parametrize("L", PAIR_LENGTHS)
-def test_query_pairs_equal_unpaired_launches(L):
+def test_query_pairs_equal_unpaired_launches(L, gaps):
     """Affine queries that share their targets are scored two per launch row
     (query 2y in the low, 2y + 1 in the high half of every word); the scores
     equal the one-query-per-row launch in both lane layouts, with an odd
-    query count and with one half of a pair outside the launch width."""
+    query count and with one half of a pair outside the launch width -- at
+    msa()'s gaps (kernels with them built in) and at others."""
     from sseqs_b200 import batched, dbtools, tune
     _, db = _db()
     b = db.batches[0]
@@ -139,7 +141,7 @@ def test_query_pairs_equal_unpaired_launches(L):
     enc, buf, lens = _pack(queries)
     lens[3] = 32 * tpt + 1             # another width: not scored in either form
     n = b.n_segments - 2
-    kw = dict(affine=True, g0=1, n_targets=n, skip=1, gap_a=11, gap_b=1)
+    kw = dict(affine=True, g0=1, n_targets=n, skip=1, gap_a=gaps[0], gap_b=gaps[1])
     before = tune.get_variant(3, tpt), tune.get_query_pairing(tpt)
     try:
         tune.set_query_pairing(tpt, False)

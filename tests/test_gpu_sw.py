@@ -51,6 +51,14 @@ def test_sw_ops_match_oracle(Lq):
     sp = (starts + 1).astype(np.int32)
     aff2 = S.sw_cuda_affine(qd, gd, ad, _dev(sp), 11, 1).cpu().numpy()
     np.testing.assert_array_equal(aff2, O.sw_affine(q, good, ascii, sp, 11, 1, NT))
+    # gaps other than msa()'s run the kernels that read them from the
+    # arguments (msa()'s own run the twins with them built in)
+    sub = good[: max(1, len(good) // 3)]
+    sd3 = _dev(sub)
+    lin4 = S.sw_cuda_blosum62(qd, sd3, ad, sd, gap_penalty_param=-4).cpu().numpy()
+    np.testing.assert_array_equal(lin4, O.sw_linear(q, sub, ascii, starts, -4, NT))
+    aff52 = S.sw_cuda_affine(qd, sd3, ad, sd, 5, 2).cpu().numpy()
+    np.testing.assert_array_equal(aff52, O.sw_affine(q, sub, ascii, starts, 5, 2, NT))
 
 
 # one query length per stripe width 1..32 (the reference's kernels L = 32..1024,
@@ -253,6 +261,10 @@ def test_scan_both_equals_two_scans(Lq, wide):
                                                    gap_a=-2), rtol=0, atol=0)
         torch.testing.assert_close(aff2, S.sw_scan(qd, ad, dd, affine=True, good_idx=gd, skip=0,
                                                    gap_a=7, gap_b=2), rtol=0, atol=0)
+        np.testing.assert_array_equal(lin2.cpu().numpy(),
+                                      O.sw_linear(q, idx, ascii, delim, -2, NT))
+        np.testing.assert_array_equal(aff2.cpu().numpy(),
+                                      O.sw_affine(q, idx, ascii, delim, 7, 2, NT))
     finally:
         v.restore()
 
