@@ -113,9 +113,9 @@ class ClockSampler:
 
 # -------------------------------------------------------------- GPU side
 # DRAM traffic of the affine score kernel per target residue, from its ncu
-# capture at 1M sequences, stripe width 27 (382.5 MB read + 7.6 MB written,
+# capture at 1M sequences, stripe width 27 (381.9 MB read + 10.0 MB written,
 # 372.7M residues)
-TRAFFIC_BYTES_PER_RESIDUE = (382.48704e6 + 7.58784e6) / 372662216
+TRAFFIC_BYTES_PER_RESIDUE = (381.879296e6 + 10.014464e6) / 372662216
 
 
 def build_database(queries, db_seqs, seed=0):
@@ -1019,12 +1019,12 @@ def bench_b200(args):
             "unit": "Gop/s",
             "frac": round(achieved / alu_peak, 4),
             # DRAM bytes of one affine launch (one database batch): the ncu
-            # capture of this kernel on a 1M-sequence batch read 382.5 MB and
-            # wrote 7.6 MB for 372.7M residues, i.e. ~1.05 B per residue,
+            # capture of this kernel on a 1M-sequence batch read 381.9 MB and
+            # wrote 10.0 MB for 372.7M residues, i.e. ~1.05 B per residue,
             # scaled here to the residues of an average batch of this database
             "traffic": int(TRAFFIC_BYTES_PER_RESIDUE * res_cells / max(1, len(db.batches))),
             "traffic_source": "ncu dram__bytes_read+write of the affine launch at 1M sequences "
-                              "(390.1 MB / 372.7M residues), scaled to an average batch",
+                              "(391.9 MB / 372.7M residues), scaled to an average batch",
             "algorithmic_bytes": int(res_cells / max(1, len(db.batches))),
             "ops_model": "3.5 ALU-pipe DPX int16x2 instructions per 2 cells (affine kernel)",
             "peak_source": "sseqs_dpx_peak measured in this run: ALU-pipe int16x2 DPX issue rate",
