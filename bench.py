@@ -756,11 +756,20 @@ def bench_serving_scale(args):
     del pairs
     torch.cuda.empty_cache()
     t2 = time.time()
-    index = learned.LearnedIndex(model, db)
+    index = learned.LearnedIndex(model, db, dim=args.index_dim)
     torch.cuda.synchronize()
     t3 = time.time()
     sweep = serving_sweep(index, SWEEP_RATES, args.sweep_seconds)
     sweep["exact_pipeline_saturation"] = exact_saturation(db)
+    # recall of the exhaustive search's top-1000 for queries with planted
+    # homologs (each query has 0.05% of every shard)
+    M = importlib.import_module("sseqs_b200.msa")
+    rec = []
+    for q in queries[:args.scale_recall_queries]:
+        ex = M.search([q], db, num_msas=TOP_K, top_fft=1, top_sw=1, top_sw_affine=TOP_K)[0]
+        got = index.search([q], n_cand=32768, top=TOP_K)[0]
+        want = {(r[1], r[2]) for r in ex[:1000]}
+        rec.append(len(want & {(r[1], r[2]) for r in got[:1000]}) / max(1, len(want)))
     best = max(r["queries_per_s"] for r in sweep["rates"])
     free, total = torch.cuda.mem_get_info()
     out = {
@@ -771,8 +780,10 @@ def bench_serving_scale(args):
         "config": {"workload": "serving at the benchmark's serving scale",
                    "db_sequences": int(args.serving_scale), "db_residues": int(n_res),
                    "db_shards": shard, "index_bytes": int(index.codes.numel()),
-                   "device_bytes_in_use": int(total - free)},
+                   "index_dim": index.dim, "device_bytes_in_use": int(total - free)},
         "serving_sweep": sweep,
+        "recall_of_exact_top1000": [round(r, 4) for r in rec],
+        "recall_candidates_per_query": 32768,
         "seconds_build_db": round(t1 - t0, 1), "seconds_train": round(t2 - t1, 1),
         "seconds_index": round(t3 - t2, 1),
     }
@@ -1209,6 +1220,12 @@ def main():
                     help="instead of the benchmark: the learned prefilter at its stated size "
                          "(training on --learned-pairs pairs, --learned-queries timed queries, "
                          "recall over --recall-queries queries with planted homologs)")
+    ap.add_argument("--index-dim", type=int, default=256, choices=(128, 256),
+                    help="--serving-scale: width of the FP8 index codes (128: the embeddings "
+                         "projected onto their 128 leading principal directions)")
+    ap.add_argument("--scale-recall-queries", type=int, default=2,
+                    help="--serving-scale: planted-homolog queries whose recall of the exact "
+                         "top-1000 is measured (each needs one exhaustive search)")
     ap.add_argument("--recall-queries", type=int, default=128,
                     help="queries with planted homologs whose recall --learned-scale reports")
     ap.add_argument("--recall-homologs", type=int, default=500,

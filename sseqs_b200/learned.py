@@ -488,15 +488,48 @@ def train(model: Embedder, pairs: PairSet, *, queries_per_step: int = 32,
 
 
 # ----------------------------------------------------------------- search
-class LearnedIndex:
-    """FP8 codes of every database segment, resident in HBM."""
+def principal_directions(emb: torch.Tensor, k: int, max_rows: int = 1 << 20) -> torch.Tensor:
+    """The k leading eigenvectors [256, k] (fp32, on emb's device) of the
+    second-moment matrix of unit embeddings (rows of ``emb``, evenly
+    subsampled to at most ``max_rows``): the k-dimensional subspace that
+    keeps the most of their dot products."""
+    step = max(1, emb.shape[0] // max_rows)
+    x = emb[::step].to(torch.float64)
+    c = (x.T @ x).cpu().numpy() / max(1, x.shape[0])
+    w, v = np.linalg.eigh(c)                       # ascending eigenvalues
+    top = v[:, np.argsort(w)[::-1][:k]]
+    return torch.from_numpy(np.ascontiguousarray(top)).to(torch.float32).to(emb.device)
 
-    def __init__(self, model: Embedder, db, chunk: int = 32768):
-        self.model, self.db = model, db
+
+def project(emb: torch.Tensor, proj: torch.Tensor) -> torch.Tensor:
+    """Rows of ``emb`` projected by ``proj`` and scaled back to unit norm."""
+    y = emb @ proj
+    return (y / y.norm(dim=1, keepdim=True).clamp_min(1e-12)).contiguous()
+
+
+class LearnedIndex:
+    """FP8 codes of every database segment, resident in HBM.
+
+    ``dim`` is the code width: 256 (the embedding itself) or 128 (its
+    projection onto the 128 leading principal directions of the database's
+    embeddings, renormalised), which halves the index (200M segments: 25.6
+    instead of 51.2 GB).  The selection kernel reads 256-byte rows; a
+    128-wide index is read as rows of two consecutive codes, against two
+    query columns per query, [q, 0] and [0, q], whose scores are those of the
+    even and the odd code of every pair."""
+
+    def __init__(self, model: Embedder, db, chunk: int = 32768, dim: int = D):
+        if dim not in (D, D // 2):
+            raise ValueError(f"code width {dim}: 256 or 128")
+        self.model, self.db, self.dim = model, db, dim
         counts = [b.n_segments for b in db.batches]
         self.cum = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         n = int(self.cum[-1])
-        self.codes = torch.empty((max(n, 1), D), dtype=torch.uint8, device=db.device)
+        # a 128-wide index holds an even number of rows (the spare one all
+        # zero), so that it can be read as 256-byte rows
+        rows = max(n, 1) if dim == D else max(n + (n & 1), 2)
+        self.codes = torch.zeros((rows, dim), dtype=torch.uint8, device=db.device)
+        self.proj = None
         L = lib()
         for bi, b in enumerate(db.batches):
             if b.n_segments == 0:
@@ -504,6 +537,10 @@ class LearnedIndex:
             # a whole batch per call: its chunks are queued back to back
             emb = model.embed(b.ascii, b.offsets[:b.n_segments], b.lengths[:b.n_segments],
                               chunk=chunk)
+            if dim < D:
+                if self.proj is None:
+                    self.proj = principal_directions(emb, dim)
+                emb = project(emb, self.proj)
             row = int(self.cum[bi])
             check(L.sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE,
                                         self.codes[row:row + b.n_segments].data_ptr(),
@@ -512,17 +549,30 @@ class LearnedIndex:
         self.n = n
 
     def query_codes(self, enc_queries) -> torch.Tensor:
-        """FP8 codes [nq, 256] of queries given as ASCII strings."""
+        """FP8 codes [nq, dim] of queries given as ASCII strings."""
         dev = self.db.device
         buf = "".join(q + "@" for q in enc_queries).encode()
         ascii = torch.from_numpy(np.frombuffer(buf, np.uint8).copy()).to(dev)
         lens = torch.tensor([len(q) for q in enc_queries], dtype=torch.int64, device=dev)
         offs = torch.cumsum(lens + 1, 0) - (lens + 1)
         emb = self.model.embed(ascii, offs, lens)
-        codes = torch.empty((len(enc_queries), D), dtype=torch.uint8, device=dev)
+        if self.dim < D:
+            emb = project(emb, self.proj)
+        codes = torch.empty((len(enc_queries), self.dim), dtype=torch.uint8, device=dev)
         check(lib().sseqs_quantize_e4m3(ptr(emb), emb.numel(), CODE_SCALE, ptr(codes),
                                         stream_ptr()), "quantize")
         return codes
+
+    def _wide(self, qcodes: torch.Tensor) -> torch.Tensor:
+        """256-byte query rows: the codes themselves, or for a 128-wide index
+        [q, 0] and [0, q] per query (rows 2i and 2i + 1)."""
+        if self.dim == D:
+            return qcodes.contiguous()
+        nq = qcodes.shape[0]
+        w = torch.zeros((2 * nq, D), dtype=torch.uint8, device=qcodes.device)
+        w[0::2, :self.dim] = qcodes
+        w[1::2, self.dim:] = qcodes
+        return w
 
     def _select(self, qcodes: torch.Tensor, n_cand: int, sample: int, factor: float,
                 cap_factor: int):
@@ -537,20 +587,34 @@ class LearnedIndex:
         # evenly spaced rows in integer arithmetic (float32 cannot hold
         # every row index of a 20M-row index)
         rows = torch.arange(S, dtype=torch.int64, device=dev) * (self.n - 1) // max(S - 1, 1)
-        samp = self.codes[rows].contiguous()
+        samp = self.codes[rows]
+        qwide = self._wide(qcodes)
+        if self.dim < D:
+            # zero-padded to 256 bytes: [q, 0] . [s, 0] = q . s
+            samp = torch.cat([samp, torch.zeros_like(samp)], dim=1)
+            qs = qwide[0::2].contiguous()
+        else:
+            qs = qwide
+        samp = samp.contiguous()
         dense = torch.empty((nq, S), dtype=torch.float32, device=dev)
-        check(L.sseqs_score_dense(ptr(qcodes), nq, ptr(samp), S, ptr(dense), stream_ptr()),
+        check(L.sseqs_score_dense(ptr(qs), nq, ptr(samp), S, ptr(dense), stream_ptr()),
               "score_dense")
         k_s = max(1, min(S, int(math.ceil(factor * n_cand * S / max(self.n, 1)))))
         tau = torch.empty(nq, dtype=torch.float32, device=dev)
         check(L.sseqs_kth_largest_rows(ptr(dense), nq, S, k_s, ptr(tau), stream_ptr()),
               "kth_largest")
+        # the selection over 256-byte rows: query columns and index rows as
+        # the kernel reads them
+        half = self.dim < D
+        ncol = qwide.shape[0]
+        tau_c = tau.repeat_interleave(2) if half else tau
+        n_rows = self.codes.shape[0] // 2 if half else self.n
         cap = int(min(self.n, max(n_cand * cap_factor, 1024)))
         while True:
-            count = torch.zeros(nq, dtype=torch.int32, device=dev)
-            cand = torch.empty((nq, cap), dtype=torch.int64, device=dev)
-            cs = torch.empty((nq, cap), dtype=torch.float32, device=dev)
-            check(L.sseqs_score_select(ptr(qcodes), nq, ptr(self.codes), self.n, ptr(tau),
+            count = torch.zeros(ncol, dtype=torch.int32, device=dev)
+            cand = torch.empty((ncol, cap), dtype=torch.int64, device=dev)
+            cs = torch.empty((ncol, cap), dtype=torch.float32, device=dev)
+            check(L.sseqs_score_select(ptr(qwide), ncol, ptr(self.codes), n_rows, ptr(tau_c),
                                        ptr(count), ptr(cand), ptr(cs), cap, stream_ptr()),
                   "score_select")
             cnt = to_host(count)
@@ -561,7 +625,32 @@ class LearnedIndex:
             if int(cnt.max(initial=0)) <= cap or cap >= self.n:
                 break
             cap = int(min(self.n, 2 * int(cnt.max())))
-        return cand, cs, cnt, cap
+        if not half:
+            return cand, cs, cnt, cap
+        return self._merge_columns(cand, cs, cnt, cap)
+
+    def _merge_columns(self, cand, cs, cnt, cap):
+        """The two query columns of a 128-wide index back to one list per
+        query: row r of column 2i is code 2r, of column 2i + 1 code 2r + 1;
+        the spare zero row is dropped.  Returns (cand [nq, 2 cap], scores,
+        host counts, 2 cap), each query's entries first in its row."""
+        dev = cand.device
+        ncol = cand.shape[0]
+        nq = ncol // 2
+        took = torch.from_numpy(np.minimum(cnt, cap).astype(np.int64)).to(dev)
+        live = torch.arange(cap, device=dev)[None, :] < took[:, None]
+        col = torch.arange(ncol, device=dev)
+        code = 2 * cand + (col & 1)[:, None]
+        keep = live & (code < self.n)
+        qid = (col // 2)[:, None].expand(ncol, cap)[keep]         # query-major
+        code, score = code[keep], cs[keep]
+        cntq = torch.bincount(qid, minlength=nq)
+        pos = torch.arange(qid.numel(), device=dev) - (torch.cumsum(cntq, 0) - cntq)[qid]
+        out = torch.zeros((nq, 2 * cap), dtype=torch.int64, device=dev)
+        out_s = torch.zeros((nq, 2 * cap), dtype=torch.float32, device=dev)
+        out[qid, pos] = code
+        out_s[qid, pos] = score
+        return out, out_s, to_host(cntq).astype(np.int64), 2 * cap
 
     def candidates_flat(self, qcodes: torch.Tensor, n_cand: int, sample: int = 8192,
                         factor: float = 2.5, cap_factor: int = 8):

@@ -320,7 +320,8 @@ def test_score_select_paths(nq, n, path):
             assert (cs[i, :c] - ref[i, rows]).abs().max().item() < 1e-3
 
 
-def test_learned_search_reports_exact_scores():
+@pytest.mark.parametrize("dim", [256, 128])
+def test_learned_search_reports_exact_scores(dim):
     from sseqs_b200 import dbtools, learned, select
     from sseqs_b200.database import Database
     sw = importlib.import_module("sseqs_b200.sw")
@@ -332,7 +333,8 @@ def test_learned_search_reports_exact_scores():
     syn = dbtools.synthetic_db([q0], 4000, 0.02, (0.5, 0.95), seed=11, device="cpu",
                                chunk_bytes=150_000)
     db = Database(syn.chunks, bs=150_000)
-    idx = learned.LearnedIndex(model, db, chunk=1000)
+    idx = learned.LearnedIndex(model, db, chunk=1000, dim=dim)
+    assert idx.codes.shape[1] == dim
     hits = idx.search([q0], n_cand=300, top=50)[0]
     assert hits
     enc = sw.encode_query(q0)
@@ -461,3 +463,40 @@ def test_pack_segments_copies_every_window():
     want = np.concatenate([np.concatenate([host[p][s:s + l], [64]]).astype(np.uint8)
                            for p, s, l in zip(part, src, ln)])
     assert np.array_equal(out.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("path", [1, 0])    # 1: tcgen05 kind::f8f6f4, 0: mma.sync
+def test_half_width_index_selects_by_its_codes(path):
+    """A 128-wide index (read by the selection kernel as 256-byte rows of two
+    codes, against [q, 0] and [0, q]): every returned row is a real code row
+    (the spare zero row never), reported once, with the fp32 dot product of
+    the query's and the row's 128-byte codes within 1e-3, and every row more
+    than 1e-3 above the lowest reported score is returned."""
+    from sseqs_b200 import _lib, dbtools, learned
+    db = _ragged_db(seed=8)
+    idx = learned.LearnedIndex(learned.Embedder(seed=8), db, chunk=1000, dim=128)
+    n = idx.n
+    assert idx.codes.shape == (n + (n & 1), 128)
+    assert not idx.codes[n:].any()
+    queries = [dbtools.random_query(L, 800 + j) for j, L in enumerate([60, 250, 512, 999])]
+    codes = idx.query_codes(queries)
+    assert codes.shape == (len(queries), 128)
+    qf = codes.view(torch.float8_e4m3fn).float()
+    df = idx.codes[:n].view(torch.float8_e4m3fn).float()
+    ref = qf @ df.T
+    _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(path), "path")
+    try:
+        cand, cs, cnt, cap = idx._select(codes, 50, 8192, 2.5, 8)
+        torch.cuda.synchronize()
+    finally:
+        _lib.check(_lib.lib().sseqs_gemm_set_tensor_path(1), "path")
+    assert _gemm_error() == 0
+    for j in range(len(queries)):
+        c = int(min(cnt[j], cap))
+        assert c > 50
+        rows = cand[j, :c]
+        got = set(rows.tolist())
+        assert len(got) == c and max(got) < n
+        assert (cs[j, :c] - ref[j, rows]).abs().max().item() < 1e-3
+        low = float(cs[j, :c].min())
+        assert set(torch.nonzero(ref[j] >= low + 1e-3).flatten().tolist()) <= got

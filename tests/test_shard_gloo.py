@@ -34,7 +34,7 @@ def _worker(rank, world, port, out):
 def test_gather_hits_two_ranks():
     world = 2
     port = _free_port()
-    manager = mp.Manager()
+    manager = mp.get_context("spawn").Manager()   # no fork after torch has started threads
     out = manager.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     assert out[0] == out[1]
