@@ -546,6 +546,8 @@ class LearnedIndex:
                                         self.codes[row:row + b.n_segments].data_ptr(),
                                         stream_ptr()), "quantize")
             del emb
+        if dim < D and self.proj is None:     # no segments: any projection will do
+            self.proj = torch.eye(D, dim, dtype=torch.float32, device=db.device)
         self.n = n
 
     def query_codes(self, enc_queries) -> torch.Tensor:
