@@ -658,6 +658,21 @@ def bench_learned_scale(args):
         torch.cuda.synchronize()
         depths.append(dict(recall(hits, depth),
                            queries_per_s=round(nr / (e0.elapsed_time(e1) * 1e-3), 2)))
+    # the same embedder with a 128-wide index (the embeddings projected onto
+    # their 128 leading principal directions), at the default depth
+    del index
+    torch.cuda.empty_cache()
+    index128 = learned.LearnedIndex(model, db, dim=128)
+    index128.search_arrays(recall_qs[:4], n_cand=32768, top=TOP_K)    # warm-up
+    torch.cuda.synchronize()
+    e0.record()
+    hits = []
+    for s0 in range(0, nr, chunk):
+        hits += index128.search_arrays(recall_qs[s0:s0 + chunk], n_cand=32768, top=TOP_K)
+    e1.record()
+    torch.cuda.synchronize()
+    r128 = dict(recall(hits, 32768), queries_per_s=round(nr / (e0.elapsed_time(e1) * 1e-3), 2),
+                index_bytes=int(index128.codes.numel()))
     qps_l = len(qs) / (ms_learned * 1e-3)
     qps_lr = nr / (ms_learned_r * 1e-3)
     qps_e = nr / (ms_exact * 1e-3)
@@ -679,8 +694,9 @@ def bench_learned_scale(args):
         "recall_of_exact_top1000": r32["recall_of_exact_top1000"],
         "recall_min": r32["recall_min"],
         "recall_by_identity_band": r32["recall_by_identity_band"],
-        "scores_equal_exact": all(d["scores_equal_exact"] for d in depths),
+        "scores_equal_exact": all(d["scores_equal_exact"] for d in depths + [r128]),
         "candidate_depths": depths,
+        "index_128": r128,
         "train_loss_first_last": [hist["losses"][0][1], hist["losses"][-1][1]],
         "train_steps": hist["steps"],
         "seconds_build_db": round(t1 - t0, 1), "seconds_pairs": round(t2 - t1, 1),
