@@ -971,7 +971,7 @@ def bench_b200(args):
     gcups = total_cells / (ms * 1e-3) / 1e9
     aff_ms = [a.elapsed_time(b) for a, b in events["affine"]]
     both_ms = [a.elapsed_time(b) for a, b in events["both"]]
-    # queries of up to 672 residues score both variants in one fused launch;
+    # queries of up to 736 residues score both variants in one fused launch;
     # longer ones launch the affine kernel on its own
     aff_cells = sum(len(q) * res_cells for q in timed if not tune.fused(len(q)))
     both_cells = sum(len(q) * res_cells for q in timed if tune.fused(len(q)))
@@ -1040,7 +1040,7 @@ def bench_b200(args):
         "roofline": {
             "bound": "int-pipe (ALU, DPX)",
             "kernel": "sw_stream_kernel<affine> (dominant launch of the step; queries of more "
-                      "than 672 residues)",
+                      "than 736 residues)",
             "achieved": round(achieved / 1e9, 1),
             "peak": round(alu_peak / 1e9, 1),
             "unit": "Gop/s",
@@ -1059,7 +1059,7 @@ def bench_b200(args):
                           "peak": round(dual_peak / 1e9, 1),
                           "frac": round(aff_rate * 5.5 / 2 / dual_peak, 4),
                           "ops_model": "5.5 int16x2 instructions per 2 cells (3.5 ALU + 2 FMA)"},
-            "fused": {"kernel": "sw_stream_kernel<both> (queries of up to 672 residues)",
+            "fused": {"kernel": "sw_stream_kernel<both> (queries of up to 736 residues)",
                       "achieved": round(both_rate * 2.5 / 1e9, 1),
                       "peak": round(alu_peak / 1e9, 1),
                       "frac": round(both_rate * 2.5 / alu_peak, 4),

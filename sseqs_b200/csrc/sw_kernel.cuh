@@ -715,8 +715,9 @@ KernelInfo make_info() {
 // here).  Measured on B200 (300k-1M segments), the fused pass beat the two
 // kernels by 4-17% up to width 16 and by 5% at 20 (8 rows per fetch),
 // broke even at 27 and lost 13% at 41-48: its three states need ~200-255
-// registers there, which leaves 8 warps per SM.
-constexpr int kMaxFusedTpt = 21;
+// registers there, which leaves 8 warps per SM.  With msa()'s gaps built in
+// (1M segments): +7% at 22, +6% at 23, -2% to +2% at 25-32.
+constexpr int kMaxFusedTpt = 23;
 struct Tables {
   KernelInfo k[2][2][kModes][64];
 };

@@ -30,7 +30,7 @@ def tpt_of(query_len: int) -> int:
 
 
 MODES = ("linear", "affine", "both", "pair")
-MAX_FUSED_TPT = 21      # widths scored by the fused pass (wider: the two kernels)
+MAX_FUSED_TPT = 23      # widths scored by the fused pass (wider: the two kernels)
 
 
 def set_variant(affine, tpt: int, wide: int) -> None:

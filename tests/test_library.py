@@ -73,7 +73,7 @@ def test_batched_buckets_group_by_stripe_width():
 
 def test_score_kernel_registry_matches_dispatch_rules(built_lib):
     """The instantiated score kernels are the ones the host dispatch counts
-    on: the fused pass up to width 21 (``tune.fused``), a wide layout of its
+    on: the fused pass up to width 23 (``tune.fused``), a wide layout of its
     own for the linear kernel at widths 2-29 and for the affine and fused
     kernels at 2-16 (``tune.has_wide``; at width 1 both layouts hold 16
     words per lane).  Read from the library's registry;
@@ -81,14 +81,14 @@ def test_score_kernel_registry_matches_dispatch_rules(built_lib):
     from sseqs_b200 import _lib, tune
     L = _lib.lib()
     words = lambda mode, t, wide: L.sseqs_sw_variant_words(mode, t, wide)
-    assert tune.MAX_FUSED_TPT == 21
+    assert tune.MAX_FUSED_TPT == 23
     for t in range(1, 65):
-        assert (words(2, t, 0) > 0) == (t <= 21), t
-        assert tune.fused(32 * t) == (t <= 21)
+        assert (words(2, t, 0) > 0) == (t <= 23), t
+        assert tune.fused(32 * t) == (t <= 23)
         assert words(0, t, 0) > 0 and words(1, t, 0) > 0
         assert tune.has_wide(0, t) == (2 <= t <= 29), t
         assert tune.has_wide(1, t) == (2 <= t <= 16), t
-        if t <= 21:
+        if t <= 23:
             assert tune.has_wide(2, t) == (2 <= t <= 16), t
         # the query-pair kernel (mode 3) exists at every width, with the
         # affine kernel's layouts
