@@ -105,7 +105,7 @@ int sseqs_sw_scan(int affine, const uint8_t* query_idx, int query_len,
  * (the exact search of sseqs/msa.py:313-332 with top_sw = 1 makes both),
  * including query_len 0, where every result of both is -1.
  * Gap parameters must lie in the int16 domain, else SSEQS_ERR_UNSUPPORTED
- * (make the two calls instead).  Queries of up to 672 residues run one
+ * (make the two calls instead).  Queries of up to 736 residues run one
  * fused kernel; longer ones run the two score kernels in turn.
  * Like every single-query scan, it takes its target counter from a ring of
  * 1024 library-owned slots, one per launch: eager calls overlapping on
