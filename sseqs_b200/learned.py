@@ -16,8 +16,10 @@ for the same stage (it has no reference counterpart):
   kernels (``batched.sw_scan_queries``); the loss is the squared error of
   the embeddings' cosine.
 * ``LearnedIndex`` -- the embeddings of every database segment as FP8 e4m3
-  codes resident in HBM; a query's candidates are the rows whose code dot
-  product reaches a per-query threshold (estimated from a sample so that
+  codes resident in HBM (256 bytes per segment, or 128 after a projection
+  onto the embeddings' leading principal directions); a query's candidates
+  are the rows whose code dot product reaches a per-query threshold
+  (estimated from a sample so that
   about ``factor`` times the wanted count pass), selected inside the FP8
   GEMM's epilogue (``sseqs_score_select``), cut to the wanted count, and
   re-scored by exact affine SW.  Every reported score is an exact integer SW
