@@ -39,6 +39,16 @@ _sw = importlib.import_module("sseqs_b200.sw")
 
 HIT_WIDTH = 500           # sseqs/msa.py:183
 
+# The keys of msa(..., return_timings=True) (sseqs/msa.py:442-446).  Here
+# t_fft is the prefilter, t_topk1 its top-k, t_sw the linear and affine
+# scoring with their top-k, t_out the hit gather, t_a3m the traceback and
+# file; decompression and host-to-device copies happen once, when the
+# database is loaded, so those keys and the reference's other
+# per-batch preparation keys stay 0.
+TIMING_KEYS = ("t_dec", "t_prep1", "t_prep2", "t_fft", "t_prep_fft", "t_sw", "t_out",
+               "t_out_cpu", "t_log", "t_topk1", "t_topk2", "t_save", "t_prep_sw", "t_a3m",
+               "t_to_vram")
+
 
 @dataclass
 class BatchHits:
@@ -56,12 +66,25 @@ class BatchHits:
 
 
 class SearchStats:
-    def __init__(self):
+    """Host seconds per stage; with ``sync`` every stage waits for the GPU
+    before its clock is read (the reference's ``sync_time``)."""
+
+    def __init__(self, sync: bool = False):
         self.cells = 0
         self.stage = {}
+        self.sync = sync
 
     def add(self, key, dt):
         self.stage[key] = self.stage.get(key, 0.0) + dt
+
+    def clock(self) -> float:
+        if self.sync:
+            torch.cuda.synchronize()
+        return time.time()
+
+    def timings(self) -> dict:
+        """The reference's timings dict: every key of TIMING_KEYS."""
+        return {k: float(self.stage.get(k, 0.0)) for k in TIMING_KEYS}
 
 
 def _gather_hits(batch, g, n):
@@ -87,8 +110,14 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
         cand = None                                         # segments 1 .. nseg-2
     else:
         from . import conv
+        t0 = stats.clock() if stats is not None else 0.0
         scores = conv.prefilter_batch(query, batch, luts, fft_rank)
+        t1 = stats.clock() if stats is not None else 0.0
         cand = select.topk_indices(scores, k1)[1:-1]
+        if stats is not None:
+            stats.add("t_fft", t1 - t0)
+            stats.add("t_topk1", stats.clock() - t1)
+    t_sw0 = stats.clock() if stats is not None else 0.0
     Lq = q_enc.numel()
     k2 = n_c // top_sw
     if top_sw == 1 and tune.fused(Lq):
@@ -110,6 +139,8 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
             lin = _sw.sw_scan(q_enc, batch.ascii, batch.delim, affine=False, good_idx=cand,
                               skip=0, gap_a=-1)
         if k2 <= 0:
+            if stats is not None:
+                stats.add("t_sw", stats.clock() - t_sw0)
             return None
         if top_sw == 1:
             p2, cand2 = None, cand
@@ -142,7 +173,12 @@ def search_batch(q_enc: torch.Tensor, query: str, batch, bi: int, *, top_fft=200
     else:
         g = cand2[p3].to(torch.int32)
     pos = p3 if p2 is None else p2.long()[p3]
+    if stats is not None:
+        t_out0 = stats.clock()
+        stats.add("t_sw", t_out0 - t_sw0)
     hits, hlen = _gather_hits(batch, g, k3)
+    if stats is not None:
+        stats.add("t_out", stats.clock() - t_out0)
     return BatchHits(bi, g, aff[p3], lin[pos], hits, hlen, batch.maxlen, 0, 0, pos,
                      None if top_fft == 1 else scores)
 
@@ -245,12 +281,9 @@ def search(queries, db: Database | None = None, *, num_msas=4096, top_fft=200, t
         for bi, batch in enumerate(db.batches):
             if abs(len(query) - batch.maxlen) > dlength:   # msa.py:252
                 continue
-            t0 = time.time()
             per.append(search_batch(q_enc, query, batch, bi, top_fft=top_fft, top_sw=top_sw,
                                     top_sw_affine=top_sw_affine, fft_rank=fft_rank, luts=luts,
                                     stats=stats, timer=timer))
-            if stats is not None:
-                stats.add("t_sw", time.time() - t0)
         out.append(rank_hits(query, per, num_msas))
         if per_batch_out is not None:
             per_batch_out.append(per)
@@ -283,7 +316,7 @@ def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50
         for f in filenames:
             if f is not None and os.path.exists(f):
                 os.remove(f)
-        stats = SearchStats()
+        stats = SearchStats(sync=sync_time)
         t0 = time.time()
         per_batch = [] if save_raw != "" else None
         ranked = search(queries, db, num_msas=num_msas, top_fft=top_fft, top_sw=top_sw,
@@ -295,8 +328,10 @@ def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50
         for qi, (query, fname, rows) in enumerate(zip(queries, filenames, ranked)):
             if save_raw != "":
                 # one file, rewritten per query, as sseqs/msa.py:420-422 does
+                ts = time.time()
                 with open(save_raw, "wb") as fh:
                     pickle.dump(raw_hits(query, per_batch[qi]), fh)
+                stats.add("t_save", time.time() - ts)
             t1 = time.time()
             if fname is not None:
                 if verbose:
@@ -306,4 +341,4 @@ def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50
         if verbose:
             print(f"searched {len(queries)} queries, {sum(len(r) for r in ranked)} hits")
         if return_timings:
-            return dict(stats.stage)
+            return stats.timings()

@@ -173,8 +173,11 @@ def test_msa_writes_oracle_a3m(tmp_path):
     q, syn = _db(n_seqs=3000, seed=5)
     db = Database(syn.chunks, bs=150_000)
     f = tmp_path / "out.a3m"
-    sseqs_b200.msa(q, str(f), num_msas=200, top_fft=1, top_sw=1, top_sw_affine=200, bs=150_000,
-                   db=db, verbose=False)
+    t = sseqs_b200.msa(q, str(f), num_msas=200, top_fft=1, top_sw=1, top_sw_affine=200,
+                       bs=150_000, db=db, verbose=False, return_timings=True, sync_time=True)
+    # the reference's timings dict (sseqs/msa.py:442-446)
+    assert set(t) == set(importlib.import_module("sseqs_b200.msa").TIMING_KEYS)
+    assert t["t_sw"] > 0 and t["t_a3m"] > 0 and t["t_out"] > 0 and t["t_fft"] == 0
     rows = _oracle_search(q, _host_batches(syn, 150_000), top_fft=1, top_sw=1,
                           top_sw_affine=200)[:200]
     _, al = O.sw_affine_backtrack(q, [r[5] for r in rows])

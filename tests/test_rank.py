@@ -60,3 +60,20 @@ def test_rank_hits_empty():
                         torch.zeros(0, dtype=torch.int32), torch.zeros((0, 8), dtype=torch.uint8),
                         torch.zeros(0, dtype=torch.int32), 10, 0, 0)
     assert M.rank_hits("MKT", [empty], 10) == []
+
+
+def test_timings_have_the_reference_keys():
+    """msa(..., return_timings=True) returns the reference's dict: the keys
+    of sseqs/msa.py:442-446, seconds as floats, stages this build does not
+    have at 0."""
+    ref_keys = {"t_dec", "t_prep1", "t_prep2", "t_fft", "t_prep_fft", "t_sw", "t_out",
+                "t_out_cpu", "t_log", "t_topk1", "t_topk2", "t_save", "t_prep_sw", "t_a3m",
+                "t_to_vram"}
+    st = M.SearchStats()
+    st.add("t_sw", 0.25)
+    st.add("t_sw", 0.5)
+    st.add("t_search", 1.0)             # internal, not part of the reference's dict
+    t = st.timings()
+    assert set(t) == ref_keys
+    assert t["t_sw"] == 0.75 and t["t_fft"] == 0.0
+    assert all(isinstance(v, float) for v in t.values())
