@@ -38,6 +38,7 @@ from .to_a3m import to_a3m
 _sw = importlib.import_module("sseqs_b200.sw")
 
 HIT_WIDTH = 500           # sseqs/msa.py:183
+_last_call: dict = {}     # gpu -> thread of the last non-blocking msa() call
 
 # The keys of msa(..., return_timings=True) (sseqs/msa.py:442-446).  Here
 # t_fft is the prefilter, t_topk1 its top-k, t_sw the linear and affine
@@ -301,9 +302,15 @@ def msa(queries, filenames=None, num_msas=4096, save_raw="", verbose=True, bs=50
     returns it, as the reference does.
     """
     if not blocking:
+        # one call in flight per GPU: a new call first waits for the last one
+        # started on the same GPU (sseqs/msa.py:87-101)
+        prev = _last_call.get(gpu)
+        if prev is not None and prev.is_alive():
+            prev.join()
         t = threading.Thread(target=msa, args=(queries, filenames, num_msas, save_raw, verbose,
                                                bs, fft_rank, top_fft, top_sw, top_sw_affine,
                                                return_timings, sync_time, dlength, gpu, True, db))
+        _last_call[gpu] = t
         t.start()
         return t
     with torch.cuda.device(gpu):

@@ -186,6 +186,25 @@ def test_msa_writes_oracle_a3m(tmp_path):
     assert sum(1 for r in rows[:20] if r[3] > 100) >= 15
 
 
+def test_msa_non_blocking_runs_one_call_per_gpu(tmp_path):
+    """blocking=False returns the thread; a second call on the same GPU first
+    waits for the one before it (sseqs/msa.py:87-101), and both write the
+    same a3m as a blocking call."""
+    from sseqs_b200.database import Database
+    import sseqs_b200
+    q, syn = _db(n_seqs=2000, seed=6)
+    db = Database(syn.chunks, bs=150_000)
+    kw = dict(num_msas=100, top_fft=1, top_sw=1, top_sw_affine=100, bs=150_000, db=db,
+              verbose=False)
+    f0, f1, f2 = (tmp_path / f"{i}.a3m" for i in range(3))
+    sseqs_b200.msa(q, str(f0), **kw)
+    t1 = sseqs_b200.msa(q, str(f1), blocking=False, **kw)
+    t2 = sseqs_b200.msa(q, str(f2), blocking=False, **kw)
+    assert not t1.is_alive()
+    t2.join()
+    assert f1.read_text() == f0.read_text() == f2.read_text()
+
+
 def test_fasta_database_names_its_hits(tmp_path):
     """A FASTA file packed with its sidecar index, loaded with batches smaller
     than a chunk: every ranked hit's string lies inside the sequence its
