@@ -115,6 +115,28 @@ def encode_query(query: str, device="cuda") -> torch.Tensor:
                      device)
 
 
+def encode_seq(s: str, device="cuda") -> torch.Tensor:
+    """The sequence as int16 character codes behind one leading 0, the
+    layout sseqs/sw.py:262-265 feeds its traceback (kept for callers of that
+    helper; the traceback here takes the strings themselves)."""
+    codes = torch.tensor([0] + [ord(c) for c in s], dtype=torch.int16)
+    return codes if str(device) == "cpu" else codes.to(device)
+
+
+def pack_targets(targets: list[str], device="cuda"):
+    """Targets as an int16 [B, W] matrix of character codes, each row a 0
+    then its sequence then zeros, with int32 lengths (sequence + 1) and the
+    width W = longest + 1 (sseqs/sw.py:267-276)."""
+    W = max(len(t) for t in targets) + 1
+    T = torch.zeros((len(targets), W), dtype=torch.int16)
+    for i, t in enumerate(targets):
+        T[i, 1:len(t) + 1] = torch.tensor([ord(c) for c in t], dtype=torch.int16)
+    lens = torch.tensor([len(t) + 1 for t in targets], dtype=torch.int32)
+    if str(device) != "cpu":
+        T, lens = T.to(device), lens.to(device)
+    return T, lens, W
+
+
 def sw(query: str, targets: list[str], gap_open: int = 11, gap_extend: int = 1) -> torch.Tensor:
     """Affine score of ``query`` against each target (sseqs/sw.py:10-23).
 

@@ -88,3 +88,17 @@ def test_raw_writer_empty_and_missing_fragment():
         a3m_text_raw(q, res)
     with pytest.raises(ValueError):
         a3m_text(q, _dicts(res))
+
+
+def test_sequence_helpers_keep_the_reference_layout():
+    """encode_seq / pack_targets (sseqs/sw.py:262-276): int16 character codes
+    behind a leading 0; rows padded with zeros to the longest target + 1,
+    lengths = sequence + 1."""
+    import importlib
+    S = importlib.import_module("sseqs_b200.sw")
+    v = S.encode_seq("AC", device="cpu")
+    assert v.dtype == torch.int16 and v.tolist() == [0, 65, 67]
+    T, lens, W = S.pack_targets(["AC", "WYV", ""], device="cpu")
+    assert W == 4 and T.dtype == torch.int16 and lens.dtype == torch.int32
+    assert T.tolist() == [[0, 65, 67, 0], [0, 87, 89, 86], [0, 0, 0, 0]]
+    assert lens.tolist() == [3, 4, 1]
