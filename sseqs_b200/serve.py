@@ -156,10 +156,12 @@ class LearnedExecutor:
     def __init__(self, index, *, top_k: int = 4096, n_cand: int = 32768):
         self.index, self.top_k, self.n_cand = index, int(top_k), int(n_cand)
 
-    @staticmethod
-    def request_bytes(top_k: int, n_batches: int) -> int:
-        # candidate lists (row + score) at the selection cap, and the hits
-        return 8 * 12 * 32768 + 16 * top_k
+    def request_bytes(self, top_k: int, n_batches: int) -> int:
+        # candidate lists (row + score, 12 bytes) at the selection cap (8x the
+        # candidates), and the hits; a 128-wide index selects two columns
+        # per query and merges them into a list twice as long (4x the bytes)
+        lists = 4 if getattr(self.index, "dim", 256) < 256 else 1
+        return lists * 8 * 12 * self.n_cand + 16 * top_k
 
     def prepare(self, req: Request) -> None:
         if not 1 <= len(req.query) <= 2048:

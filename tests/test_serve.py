@@ -135,3 +135,15 @@ def test_threaded_server_with_poisson_arrivals():
     for q, r in zip(queries, reqs):
         exp = _alone(q, n_batches=3)
         assert np.array_equal(r.result.segment, exp.segment)
+
+
+def test_learned_request_bytes_follow_the_index_width():
+    """Admission by memory counts a 128-wide index's two selection columns
+    and merged list per query (4x the candidate bytes of a 256-wide one)."""
+    class Index:
+        def __init__(self, dim):
+            self.dim = dim
+    wide = serve.LearnedExecutor(Index(256), top_k=4096, n_cand=32768)
+    half = serve.LearnedExecutor(Index(128), top_k=4096, n_cand=32768)
+    assert wide.request_bytes(4096, 5) == 8 * 12 * 32768 + 16 * 4096
+    assert half.request_bytes(4096, 5) == 4 * 8 * 12 * 32768 + 16 * 4096
